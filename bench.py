@@ -1,0 +1,342 @@
+"""Benchmark of the PaScaL_POISSON_FFT solve path on B200 (libppf).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload: the 512^3 solve (periodic x,y on [0,2pi)^2, Neumann z on [0,1]
+with tanh stretching beta=1.5), right-hand side of seeded random Fourier
+modes with a |k|^-2 spectrum plus white noise.  A step is one solve of that
+problem.  `value` is the mixed-precision solve (FP32 transforms and bulk
+tridiagonal solves, FP64 low-|k| rows, FP64 7-point residual refinement) in
+whole-job solves/s with the inputs resident in HBM; its rel-L2 against the
+plain FP64 solve of the same input is checked before timing and reported.
+The plain FP64 solve (the reference's precision) is timed beside it.  `e2e`
+times the host-array C-ABI call (ppf_solve_host: H2D of f, solve, D2H of P).
+With N > 1 (torchrun) every rank solves its own 512^3 problem (independent
+problems: weak scaling, no collective on the data path).
+
+--impl reference times the CPU restatement of the reference's solve (the
+reference's own CPU build needs Fortran/MPI/FFTW, absent here) on the
+host's cores, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "512³ solves/s: mixed-prec+refine vs FP64 plain, 1 B200, ≤1e-10 rel-L2; HBM %"
+TOL = 1e-10
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, nargs=3, default=[512, 512, 512], help="n1m n2m n3m")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    lrank = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, lrank
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while running."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.rows = []
+        self.proc = None
+        self.th = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.gpu)],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+            return
+        self.th = threading.Thread(target=self._read, daemon=True)
+        self.th.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [s.strip() for s in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.th:
+            self.th.join(timeout=2)
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def measured_hbm_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def stage_bytes(p, prec_bytes, sweeps):
+    """Algorithmic bytes per stage, summed over one solve."""
+    n1, n2, n3 = p.n1m, p.n2m, p.n3m
+    N = n1 * n2 * n3
+    spec = (n1 // 2 + 1) * n2 * n3 * 2 * prec_bytes  # one half-spectrum field (periodic x,y)
+    runs = 1 + sweeps
+    return {
+        "x-forward": runs * (8 * N + spec) + sweeps * 8 * N,
+        "y-forward": runs * 2 * spec,
+        "tdma-z": runs * 2 * spec,
+        "y-inverse": runs * 2 * spec,
+        "x-inverse": runs * (spec + 8 * N) + sweeps * 8 * N,
+    }
+
+
+def load_traffic(kernel: str):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(path) as fh:
+            d = json.load(fh)
+        return d.get(kernel)
+    except (OSError, ValueError):
+        return None
+
+
+def cpu_baseline(p, threads):
+    from oracle import oracle as O
+    m = p.metrics
+    t0 = time.perf_counter()
+    O.poisson_solve(p.f, p.L1, p.L2, p.pbc, m["dmx1"], m["dmx2"], m["dmx3"], m["dx3"], nthreads=threads)
+    return time.perf_counter() - t0
+
+
+def run_reference(args, ws, rank):
+    if rank != 0:
+        return
+    from pascal_poisson_fft_b200 import workloads as W
+    threads = os.cpu_count() or 1
+    n1, n2, n3 = args.n
+    # full-size problem if (steps+warmup) solves fit the budget, else a
+    # z-slab sample of it scaled to whole solves
+    p = W.config3(n1m=n1, n2m=n2, n3m=n3)
+    t1 = cpu_baseline(p, threads)
+    budget = 150.0
+    nz_s, sample = n3, f"full {n1}x{n2}x{n3} FP64 solve per step"
+    if (args.steps + args.warmup) * t1 > budget:
+        nz_s = max(16, int(n3 * budget / ((args.steps + args.warmup) * t1)) // 16 * 16)
+        p = W.config3(n1m=n1, n2m=n2, n3m=nz_s)
+        sample = f"{n1}x{n2}x{nz_s} FP64 solve per step (z-slab sample), time scaled by {n3}/{nz_s}"
+    for _ in range(args.warmup):
+        cpu_baseline(p, threads)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        cpu_baseline(p, threads)
+    sec = (time.perf_counter() - t0) / args.steps * (n3 / nz_s)
+    value = 1.0 / sec
+    line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, PCG64)", "impl": "reference",
+            "config": {"workload": f"{n1}x{n2}x{n3} periodic-x,y Neumann-z tanh(beta=1.5) FP64 solve, CPU",
+                       "grid": [n1, n2, n3]},
+            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, ws, rank, lrank):
+    import torch
+    import pascal_poisson_fft_b200 as ppf
+    from pascal_poisson_fft_b200 import workloads as W
+
+    dev = torch.device("cuda", lrank)
+    torch.cuda.set_device(dev)
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    n1, n2, n3 = args.n
+    p = W.config3(n1m=n1, n2m=n2, n3m=n3, generate=False)
+    f = W.config3_field(p, seed=3 + rank, device=dev)
+    t = lambda a: torch.as_tensor(a, dtype=torch.float64, device=dev)
+    m = p.metrics
+    dmx1, dmx2, dmx3, dx3 = t(m["dmx1"]), t(m["dmx2"]), t(m["dmx3"]), t(m["dx3"])
+    P = torch.zeros(p.n3m + 2, p.n2m + 2, p.n1m + 2, dtype=torch.float64, device=dev)
+    P64 = torch.zeros_like(P)
+    st = torch.cuda.current_stream()
+
+    plan64 = ppf.Plan(n1, n2, n3, p.L1, p.L2, *p.pbc, precision=ppf.PPF_FP64)
+    plan64.solve(f, P64, dmx1, dmx2, dmx3, dx3)
+
+    # fewest refinement sweeps that meet the tolerance against the FP64 solve
+    sweeps, rel = None, None
+    for s in (1, 2, 3, 4):
+        planm = ppf.Plan(n1, n2, n3, p.L1, p.L2, *p.pbc, precision=ppf.PPF_MIXED, max_sweeps=s)
+        planm.solve(f, P, dmx1, dmx2, dmx3, dx3)
+        torch.cuda.synchronize()
+        rel = float(torch.linalg.vector_norm(P - P64) / torch.linalg.vector_norm(P64))
+        if rel <= TOL:
+            sweeps = s
+            break
+        planm.close()
+    if sweeps is None:
+        sweeps = 4
+
+    def timed(plan, out, k):
+        for _ in range(args.warmup):
+            plan.solve(f, out, dmx1, dmx2, dmx3, dx3)
+        if ws > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(k):
+            plan.solve(f, out, dmx1, dmx2, dmx3, dx3)
+        e1.record(st)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / k
+        if ws > 1:
+            tt = torch.tensor([ms], device=dev)
+            torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+            ms = float(tt.item())
+        return ms
+
+    clocks = ClockSampler(dev.index if "CUDA_VISIBLE_DEVICES" not in os.environ else lrank)
+    clocks.start()
+    ms_mixed = timed(planm, P, args.steps)
+    ms_fp64 = timed(plan64, P64, args.steps)
+    clk = clocks.stop()
+
+    # per-stage device times of the mixed solve (CUDA events on the solve's stream)
+    planm.stage_timing(True)
+    kst = max(3, min(args.steps, 10))
+    for _ in range(kst):
+        planm.solve(f, P, dmx1, dmx2, dmx3, dx3)
+    stages = planm.stage_times()
+    planm.stage_timing(False)
+    launches_per_solve = sum(v[1] for v in stages.values()) / kst
+    sb = stage_bytes(p, 4, sweeps)
+    dom = max(sb, key=lambda s: stages[s][0])
+    dom_ms_per_launch = stages[dom][0] / stages[dom][1]
+    dom_bytes_per_launch = sb[dom] / (stages[dom][1] / kst)
+    peak, peak_kind = measured_hbm_peak()
+    achieved = dom_bytes_per_launch / (dom_ms_per_launch * 1e-3) / 1e9
+
+    # end to end through the host-array C ABI (pinned host buffers)
+    e2e = None
+    if not args.no_e2e:
+        fh = torch.empty(f.shape, dtype=torch.float64, pin_memory=True)
+        fh.copy_(f)
+        Ph = torch.empty(P.shape, dtype=torch.float64, pin_memory=True)
+        fhn, Phn = fh.numpy(), Ph.numpy()
+        mh = [np.ascontiguousarray(m[k]) for k in ("dmx1", "dmx2", "dmx3", "dx3")]
+        for _ in range(min(args.warmup, 2)):
+            planm.solve_host(fhn, *mh, P=Phn, stream=st)
+        k2 = max(3, min(args.steps, 10))
+        if ws > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(k2):
+            planm.solve_host(fhn, *mh, P=Phn, stream=st)
+        e1.record(st)
+        torch.cuda.synchronize()
+        ms_e2e = e0.elapsed_time(e1) / k2
+        if ws > 1:
+            tt = torch.tensor([ms_e2e], device=dev)
+            torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+            ms_e2e = float(tt.item())
+        h2d = fhn.nbytes + sum(a.nbytes for a in mh)
+        e2e = {"value": ws * 1000.0 / ms_e2e, "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(Phn.nbytes), "ms_per_step": ms_e2e}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        try:
+            pc = W.config3(n1m=n1, n2m=n2, n3m=n3, generate=False)
+            pc.f = f.cpu().numpy()
+            threads = os.cpu_count() or 1
+            sec = cpu_baseline(pc, threads)
+            cpu = {"value": 1.0 / sec, "unit": "solves/s", "cores": threads, "kind": "port",
+                   "sample": f"one full {n1}x{n2}x{n3} FP64 solve of the same right-hand side"}
+        except Exception as exc:  # the baseline is reported, never the product
+            cpu = {"value": None, "unit": "solves/s", "cores": os.cpu_count(), "kind": "port",
+                   "sample": f"failed: {exc}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": ws * 1000.0 / ms_mixed, "unit": "solves/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_mixed, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64-refine",
+            "data": "synthetic (seeded PCG64 Fourier modes, |k|^-2 spectrum + white noise)",
+            "config": {"workload": f"{n1}x{n2}x{n3} Poisson, periodic x,y / Neumann z, tanh z beta=1.5, "
+                                   f"mixed FP32+FP64 refine ({sweeps} sweeps)",
+                       "grid": [n1, n2, n3], "sweeps": sweeps, "rel_l2_vs_fp64": rel,
+                       "l2_policy": "inputs larger than L2 (1 GiB FP64 field per step)",
+                       "problems_per_gpu": 1},
+            "fp64_plain": {"value": ws * 1000.0 / ms_fp64, "unit": "solves/s", "ms_per_step": ms_fp64},
+            "mixed_over_fp64": ms_fp64 / ms_mixed,
+            "stage_ms_per_solve": {k: v[0] / kst for k, v in stages.items()},
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind,
+                         "bytes_per_launch": dom_bytes_per_launch, "traffic": load_traffic(dom)},
+            "gpu_launches": int(round(launches_per_solve * args.steps)),
+            "clocks": clk,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    args = parse()
+    ws, rank, lrank = dist_env()
+    if args.impl == "reference":
+        run_reference(args, ws, rank)
+    else:
+        run_ours(args, ws, rank, lrank)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,153 @@
+/*
+ * ppf.h -- C ABI of libppf, a B200-native (sm_100a) implementation of the
+ * PaScaL_POISSON_FFT solve path: 2-D real FFT / DCT-II in x and y, batched
+ * tridiagonal solves along z, inverse transforms, mean removal and the
+ * ghost-cell update, all in hand-written CUDA kernels.
+ *
+ * Plain C types only: sizes are int, arrays are pointers, CUDA streams are
+ * passed as `void*` (a cudaStream_t, NULL = legacy default stream).  Every
+ * entry point returns an int status (PPF_OK = 0, negative on error) and
+ * never aborts; ppf_last_error() returns a message for the calling thread.
+ *
+ * Array layouts are the reference's (Fortran column-major, first index
+ * fastest):
+ *   PRHS(1:n1m, 1:n2m, 1:n3m)            right-hand side, FP64, device
+ *   P(0:n1m+1, 0:n2m+1, 0:n3m+1)          solution with ghost cells, FP64, device
+ *   dmx1(0:n1m+1) dmx2(0:n2m+1) dmx3(0:n3m+1) dx3(0:n3m+1)   metrics, FP64, device
+ * where n*m is the number of cells along an axis (the reference's n*m,
+ * n* = n*m + 1 faces).
+ */
+#ifndef PPF_H
+#define PPF_H
+
+#if defined(__GNUC__)
+#define PPF_API __attribute__((visibility("default")))
+#else
+#define PPF_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    PPF_OK = 0,
+    PPF_ERR_INVALID = -1,      /* bad argument or descriptor */
+    PPF_ERR_CUDA = -2,         /* a CUDA runtime call failed */
+    PPF_ERR_NOMEM = -3,        /* device allocation failed */
+    PPF_ERR_UNSUPPORTED = -4,  /* size/configuration outside what the kernels support */
+    PPF_ERR_STATE = -5,        /* call out of order (e.g. solve before initial) */
+    PPF_ERR_NUMERIC = -6       /* a kernel reported a non-finite pivot or hit a wait bound */
+};
+
+enum { PPF_FP64 = 0, PPF_MIXED = 1, PPF_FP32 = 2 };
+
+typedef struct ppf_plan ppf_plan;
+
+/* Plan descriptor.  Mirrors the arguments of
+ * fft_poisson_plan_cuda_create (01_Fortran/src/fft_3d_poisson.f90:70-108)
+ * at one rank, plus the precision options of this library. */
+typedef struct {
+    int n1m, n2m, n3m;         /* cells along x, y, z (n1m, n2m even) */
+    double L1, L2;             /* domain lengths along x and y (uniform spacing L/n) */
+    int pbc1, pbc2, pbc3;      /* 1 = periodic, 0 = Neumann (per axis) */
+    int precision;             /* PPF_FP64 | PPF_MIXED | PPF_FP32 */
+    int max_sweeps;            /* PPF_MIXED: FP64-residual refinement sweeps after the
+                                  first FP32 solve (0..8); <0 selects the default (2) */
+    double sweep_tol;          /* PPF_MIXED: stop refining once ||du||/||u|| < tol (0 = never) */
+    double lowk_threshold;     /* FP32 TDMA rows with lambda*dz_max^2 below this run in FP64
+                                  (<=0 selects the default 1e-3) */
+} ppf_desc;
+
+/* Create / destroy a plan on the current CUDA device.  Allocates the
+ * spectral work buffers and the twiddle / wavenumber tables. */
+PPF_API int ppf_plan_create(const ppf_desc *desc, ppf_plan **plan);
+PPF_API int ppf_plan_destroy(ppf_plan *plan);
+
+/* Solve lap(u) = f.  f_d: PRHS layout (not modified).  p_d: ghosted P layout
+ * (written: interior = solution with zero arithmetic mean, ghosts per the
+ * reference's Neumann extrapolation / periodic copy).  Metric arrays as in
+ * the header comment.  Asynchronous on `stream`; no host synchronisation.
+ * Replaces cuda_Poisson_FFT_1D (01_Fortran/src/fft_3d_poisson.f90:353-626). */
+PPF_API int ppf_solve(ppf_plan *plan, const double *f_d, double *p_d,
+              const double *dmx1_d, const double *dmx2_d,
+              const double *dmx3_d, const double *dx3_d, void *stream);
+
+/* Same as ppf_solve with host arrays: copies in, solves, copies out and
+ * synchronises `stream` before returning (the C++ driver's calling model,
+ * 00_C/examples/modules.hpp:223-232). */
+PPF_API int ppf_solve_host(ppf_plan *plan, const double *f_h, double *p_h,
+                   const double *dmx1_h, const double *dmx2_h,
+                   const double *dmx3_h, const double *dx3_h, void *stream);
+
+/* Number of refinement sweeps the last PPF_MIXED solve executed (device
+ * early exit on sweep_tol), and ||du||/||u|| of its last sweep.  Reads two
+ * device scalars (synchronises `stream`). */
+PPF_API int ppf_last_sweeps(ppf_plan *plan, int *sweeps, double *last_rel_update, void *stream);
+
+/* Per-stage device timing.  While enabled, every solve records a CUDA
+ * event after each kernel on the solve's stream; ppf_stage_times()
+ * synchronises on the recorded events, returns the accumulated
+ * milliseconds and launch counts per stage since the last call, and resets
+ * them.  Stages (the reference's NVTX ranges, fft_3d_poisson.f90:377-624):
+ * 0 z-coefficients, 1 x forward ("Poisson-F_x"), 2 y forward ("-F_y"),
+ * 3 z tridiagonal ("-TDMA-z"), 4 y inverse ("-B_y"), 5 x inverse ("-B_x"),
+ * 6 refinement gate, 7 ghost cells. */
+#define PPF_NSTAGES 8
+PPF_API int ppf_stage_timing(ppf_plan *plan, int enable);
+PPF_API int ppf_stage_times(ppf_plan *plan, double *ms, int *launches);
+
+/* Bytes of device work memory held by the plan. */
+PPF_API int ppf_plan_workspace_bytes(const ppf_plan *plan, long long *bytes);
+
+/* Batched tridiagonal solves on device arrays, system index fastest:
+ * element (sys, row) at [row * n_sys + sys].  In place: d <- x.  a, b, c
+ * are not modified (the reference overwrites c; callers that relied on
+ * that scratch content get the unmodified coefficients back instead).
+ * Replaces PaScaL_TDMA_many_solve_cuda (01_Fortran/PaScaL_TDMA/src/
+ * pascal_tdma_cuda.f90:230-269) at nprocs=1 -> tdma_many_cuda
+ * (tdmas_cuda.f90:35-102); C ABI of 00_C/PaScaL_TDMA/src/pascal_tdma.hpp:67-71. */
+PPF_API int ppf_tdma_many(const double *a, const double *b, const double *c, double *d,
+                  int n_sys, int n_row, void *stream);
+
+/* Cyclic variant (periodic systems).  Replaces
+ * PaScaL_TDMA_many_solve_cycle_cuda (pascal_tdma_cuda.f90:279-318) ->
+ * tdma_cycl_many_cuda (tdmas_cuda.f90:114-217).  n_row >= 3. */
+PPF_API int ppf_tdma_cycl_many(const double *a, const double *b, const double *c, double *d,
+                       int n_sys, int n_row, void *stream);
+
+/* Thread-local message describing the last error ("" if none). */
+PPF_API const char *ppf_last_error(void);
+
+/* Library version string. */
+PPF_API const char *ppf_version(void);
+
+/* ---------------------------------------------------------------------
+ * Reference-shaped entry points (one active plan per process, like the
+ * module-global p_poi of 01_Fortran/src/fft_3d_poisson.f90:43-59).  These
+ * are what the Fortran iso_c_binding shim binds.
+ * ------------------------------------------------------------------- */
+
+/* fft_poisson_plan_cuda_create (fft_3d_poisson.f90:70-108) at one rank:
+ * n1,n2,n3 are face counts (cells + 1), n*sub = n* at one rank.  The MPI
+ * ranks/communicators and CUDA thread shapes of the reference have no
+ * meaning here and are not taken; np1=np2=np3=1 is implied. */
+PPF_API int ppf_fft_poisson_plan_cuda_create(int n1, int n2, int n3,
+                                     double L1, double L2, double L3,
+                                     int pbc1, int pbc2, int pbc3);
+/* cuda_Poisson_FFT_initial (fft_3d_poisson.f90:110-121). */
+PPF_API int ppf_cuda_poisson_fft_initial(void);
+/* cuda_Poisson_FFT_1D (fft_3d_poisson.f90:353-626): PRHS_d is read only. */
+PPF_API int ppf_cuda_poisson_fft_1d(double *PRHS_d, double *P_d,
+                            const double *dmx1_d, const double *dmx2_d,
+                            const double *dmx3_d, const double *dx3_d);
+/* cuda_Poisson_FFT_clean (fft_3d_poisson.f90:123-130). */
+PPF_API int ppf_cuda_poisson_fft_clean(void);
+/* Selects the precision of the module-global plan before
+ * ppf_cuda_poisson_fft_initial (default PPF_FP64, the reference's). */
+PPF_API int ppf_cuda_poisson_fft_set_precision(int precision, int max_sweeps);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PPF_H */

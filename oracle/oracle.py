@@ -1,0 +1,136 @@
+"""ctypes front end of the CPU oracle (test infrastructure only).
+
+Loads ``oracle/_build/libppf_oracle.so`` (built by ``oracle/Makefile``) and
+exposes numpy-level helpers.  Only tests/, ``__graft_entry__.smoke()`` and
+bench.py's CPU-baseline leg import this module; the product path never does.
+
+Array conventions follow the reference (Fortran column-major, first index
+fastest).  numpy arrays here are C-ordered with the axes reversed, i.e. a
+field f(1:n1m,1:n2m,1:n3m) is an ndarray of shape (n3m, n2m, n1m).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+_REF = None
+
+_dp = ctypes.POINTER(ctypes.c_double)
+
+
+def build() -> None:
+    """Compile the oracle (and the reference TDMA when its tree is present)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def _ptr(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_dp)
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "_build", "libppf_oracle.so")
+        if not os.path.exists(path):
+            build()
+        L = ctypes.CDLL(path)
+        L.ora_mesh.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_double,
+                               ctypes.c_int, _dp, _dp, _dp]
+        L.ora_wavenumbers.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                      ctypes.c_int, ctypes.c_int, _dp, _dp]
+        L.ora_tdma_many.argtypes = [_dp, _dp, _dp, _dp, ctypes.c_int, ctypes.c_int]
+        L.ora_tdma_cycl_many.argtypes = [_dp, _dp, _dp, _dp, ctypes.c_int, ctypes.c_int]
+        L.ora_fft_c2c.argtypes = [_dp, ctypes.c_int, ctypes.c_int]
+        L.ora_fft_c2c.restype = ctypes.c_int
+        L.ora_poisson_solve.argtypes = [ctypes.c_int] * 3 + [ctypes.c_double] * 2 + [ctypes.c_int] * 3 + \
+            [_dp, _dp, _dp, _dp, _dp, _dp, ctypes.c_int, ctypes.c_int]
+        L.ora_poisson_solve.restype = ctypes.c_int
+        L.ora_fill_ghosts.argtypes = [ctypes.c_int] * 6 + [_dp, _dp, _dp, _dp]
+        L.ora_residual.argtypes = [ctypes.c_int] * 3 + [ctypes.c_double] * 2 + [ctypes.c_int] * 2 + \
+            [_dp, _dp, _dp, _dp, _dp]
+        _LIB = L
+    return _LIB
+
+
+def ref_tdmas():
+    """The reference's own 00_C/PaScaL_TDMA/src/tdmas.cpp, compiled by
+    oracle/Makefile into oracle/_ref/libref_tdmas.so.  None when absent."""
+    global _REF
+    if _REF is None:
+        path = os.path.join(_HERE, "_ref", "libref_tdmas.so")
+        if not os.path.exists(path):
+            return None
+        L = ctypes.CDLL(path)
+        for name in ("tdma_many", "tdma_cycl_many"):
+            getattr(L, name).argtypes = [_dp, _dp, _dp, _dp, ctypes.c_int, ctypes.c_int]
+        L.tdma_single.argtypes = [_dp, _dp, _dp, _dp, ctypes.c_int]
+        L.tdma_cycl_single.argtypes = [_dp, _dp, _dp, _dp, ctypes.c_int]
+        _REF = L
+    return _REF
+
+
+def mesh(nm: int, L: float, uniform: bool, gamma: float, pbc: bool):
+    """Faces x(0:nm+1), widths dx(0:nm+1), spacings dmx(0:nm+1)."""
+    x = np.zeros(nm + 2)
+    dx = np.zeros(nm + 2)
+    dmx = np.zeros(nm + 2)
+    lib().ora_mesh(nm, L, int(uniform), gamma, int(pbc), _ptr(x), _ptr(dx), _ptr(dmx))
+    return x, dx, dmx
+
+
+def wavenumbers(n1m, n2m, L1, L2, pbc1, pbc2):
+    kx = np.zeros(n1m)
+    ky = np.zeros(n2m)
+    lib().ora_wavenumbers(n1m, n2m, L1, L2, int(pbc1), int(pbc2), _ptr(kx), _ptr(ky))
+    return kx, ky
+
+
+def tdma_many(a, b, c, d, cyclic=False):
+    """In-place batched Thomas, arrays shaped (n_row, n_sys) (system fastest)."""
+    n_row, n_sys = d.shape
+    fn = lib().ora_tdma_cycl_many if cyclic else lib().ora_tdma_many
+    fn(_ptr(a), _ptr(b), _ptr(c), _ptr(d), n_sys, n_row)
+
+
+def fft_c2c(x: np.ndarray, sign: int) -> np.ndarray:
+    y = np.ascontiguousarray(x, dtype=np.complex128).copy()
+    lib().ora_fft_c2c(y.view(np.float64).ctypes.data_as(_dp), y.size, sign)
+    return y
+
+
+def poisson_solve(f: np.ndarray, L1: float, L2: float, pbc, dmx1, dmx2, dmx3, dx3,
+                  cpu_fft1_imag_zero: bool = True, nthreads: int = 0) -> np.ndarray:
+    """One-rank restatement of cuda_Poisson_FFT_1D.  f has shape (n3m, n2m, n1m);
+    returns the ghosted P of shape (n3m+2, n2m+2, n1m+2)."""
+    n3m, n2m, n1m = f.shape
+    f = np.ascontiguousarray(f, dtype=np.float64)
+    P = np.zeros((n3m + 2, n2m + 2, n1m + 2))
+    arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (dmx1, dmx2, dmx3, dx3)]
+    rc = lib().ora_poisson_solve(n1m, n2m, n3m, L1, L2, int(pbc[0]), int(pbc[1]), int(pbc[2]),
+                                 _ptr(f), _ptr(P), *[_ptr(a) for a in arrs],
+                                 int(cpu_fft1_imag_zero), int(nthreads))
+    if rc != 0:
+        raise ValueError(f"ora_poisson_solve rejected the problem (rc={rc})")
+    return P
+
+
+def fill_ghosts(P: np.ndarray, pbc, dmx1, dmx2, dmx3) -> None:
+    n3, n2, n1 = P.shape
+    arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (dmx1, dmx2, dmx3)]
+    lib().ora_fill_ghosts(n1 - 2, n2 - 2, n3 - 2, int(pbc[0]), int(pbc[1]), int(pbc[2]),
+                          _ptr(P), *[_ptr(a) for a in arrs])
+
+
+def residual(f, P, L1, L2, pbc, dmx3, dx3) -> np.ndarray:
+    n3m, n2m, n1m = f.shape
+    r = np.zeros_like(f)
+    lib().ora_residual(n1m, n2m, n3m, L1, L2, int(pbc[0]), int(pbc[1]),
+                       _ptr(np.ascontiguousarray(f)), _ptr(np.ascontiguousarray(P)),
+                       _ptr(np.ascontiguousarray(dmx3)), _ptr(np.ascontiguousarray(dx3)), _ptr(r))
+    return r

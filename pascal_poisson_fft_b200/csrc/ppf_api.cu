@@ -1,0 +1,588 @@
+// ppf_api.cu -- plans, solve orchestration and the C ABI of libppf.
+#include "../../include/ppf.h"
+#include "ppf_kernels.cuh"
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <vector>
+
+using namespace ppf;
+
+namespace {
+
+thread_local char g_err[512] = "";
+
+int fail(int code, const char* fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char* where)
+{
+    return fail(PPF_ERR_CUDA, "%s: %s", where, cudaGetErrorString(e));
+}
+
+#define PPF_CK(call)                                          \
+    do {                                                      \
+        cudaError_t e_ = (call);                              \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #call);   \
+    } while (0)
+
+const long double PI_L = 3.141592653589793238462643383279502884L;
+
+// e^{-2 pi i k num/den} accurately (long double argument reduction)
+void cexp_tab(int count, long double num, long double den, std::vector<double>& out)
+{
+    out.resize(2 * (size_t)count);
+    for (int k = 0; k < count; ++k) {
+        long double a = -2.0L * PI_L * (long double)k * num / den;
+        out[2 * k] = (double)cosl(a);
+        out[2 * k + 1] = (double)sinl(a);
+    }
+}
+
+bool factor(int n, FftSched& s)
+{
+    s.n = n;
+    s.npass = 0;
+    int m = n;
+    if (n < 1) return false;
+    const int order[5] = { 8, 4, 2, 3, 5 };
+    for (int r : order) {
+        while (m % r == 0 && m > 1) {
+            if (s.npass >= 12) return false;
+            s.radix[s.npass++] = r;
+            m /= r;
+        }
+    }
+    if (n == 1) { s.radix[0] = 2; s.npass = 0; }
+    return m == 1;
+}
+
+// modified wavenumbers, fft_3d_poisson.f90:288-351
+double wn_dct(int m, int n, double h)
+{
+    const double PI = 3.141592653589793238462643383279502884;
+    double s = std::sin(0.5 * (double)m * PI / (double)n);
+    return 4.0 * (s * s) / (h * h);
+}
+double wn_fft(int m, int n, double h)
+{
+    const double PI = 3.141592653589793238462643383279502884;
+    return 2.0 * (1.0 - std::cos(2.0 * (double)m * PI / (double)n)) / (h * h);
+}
+
+}  // namespace
+
+struct ppf_plan {
+    ppf_desc d{};
+    int dev = 0;
+    Geom g{};
+    bool xdct = false, ydct = false, cplx = true;
+    int ykind = Y_C2C;
+    // spectral buffers: A after the x pass, B after the y pass
+    long a_pitch = 0;      // elements of A's row type (complex for periodic x, real for DCT x)
+    long b_pitch = 0;      // elements of B's row type
+    int ycols = 0;         // complex columns the y pass walks
+    int mx = 0, my = 0;    // system grid
+    size_t elem = 8;       // sizeof(T) of the spectral data
+    void* A = nullptr;
+    void* B = nullptr;
+    size_t a_bytes = 0, b_bytes = 0;
+    double* lamx = nullptr;
+    double* lamy = nullptr;
+    double* am = nullptr;
+    double* ap = nullptr;
+    double* scal = nullptr;    // [0] dzmax2, [1..2] norms, [3] last_rel
+    int* flags = nullptr;      // [0] skip, [1] sweeps_done, [2] err
+    void* tw = nullptr;        // twiddle tables (type T)
+    size_t tw_off[5] = {};     // element offsets: x half, x n, x dct, y n, y dct
+    FftSched sx{}, sy{};
+    double scale = 1.0;
+    // device staging of ppf_solve_host (allocated on first use)
+    double* f_dev = nullptr;
+    double* p_dev = nullptr;
+    double* m_dev = nullptr;
+    // per-stage timing (ppf_stage_timing)
+    bool timing = false;
+    std::vector<std::pair<int, cudaEvent_t>> marks;   // stage id (-1 = start), event
+};
+
+namespace {
+
+template <typename T>
+int upload_twiddles(ppf_plan* p)
+{
+    const int nx = p->g.nx, ny = p->g.ny;
+    std::vector<double> xh, xn, xd, yn, yd;
+    cexp_tab(nx / 2, 1, nx / 2, xh);
+    cexp_tab(nx, 1, nx, xn);
+    cexp_tab(nx, 1, 4.0L * nx, xd);   // e^{-i pi k/(2 nx)}
+    cexp_tab(ny, 1, ny, yn);
+    cexp_tab(ny, 1, 4.0L * ny, yd);   // e^{-i pi k/(2 ny)}
+    std::vector<T> all;
+    const std::vector<double>* parts[5] = { &xh, &xn, &xd, &yn, &yd };
+    size_t off = 0;
+    for (int i = 0; i < 5; ++i) {
+        p->tw_off[i] = off / 2;
+        for (double v : *parts[i]) all.push_back((T)v);
+        off += parts[i]->size();
+        while (off % 4) { all.push_back((T)0); ++off; }  // keep 16-byte alignment of every table
+    }
+    PPF_CK(cudaMalloc(&p->tw, all.size() * sizeof(T)));
+    PPF_CK(cudaMemcpy(p->tw, all.data(), all.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return PPF_OK;
+}
+
+void drop_marks(ppf_plan* p)
+{
+    for (auto& m : p->marks) cudaEventDestroy(m.second);
+    p->marks.clear();
+}
+
+// records an event after a stage's launch when timing is enabled
+void mark(ppf_plan* p, int stage, cudaStream_t st)
+{
+    if (!p->timing) return;
+    cudaEvent_t ev;
+    if (cudaEventCreate(&ev) != cudaSuccess) return;
+    cudaEventRecord(ev, st);
+    p->marks.emplace_back(stage, ev);
+}
+
+void free_plan(ppf_plan* p)
+{
+    if (!p) return;
+    drop_marks(p);
+    void* ptrs[] = { p->A, p->B, p->lamx, p->lamy, p->am, p->ap, p->scal, p->flags, p->tw,
+                     p->f_dev, p->p_dev, p->m_dev };
+    for (void* q : ptrs)
+        if (q) cudaFree(q);
+    delete p;
+}
+
+int validate(const ppf_desc* d)
+{
+    if (!d) return fail(PPF_ERR_INVALID, "null descriptor");
+    if (d->n1m < 2 || d->n2m < 2 || d->n3m < 3)
+        return fail(PPF_ERR_INVALID, "grid %dx%dx%d too small (need n1m,n2m >= 2, n3m >= 3)", d->n1m, d->n2m, d->n3m);
+    if ((d->n1m & 1) || (d->n2m & 1))
+        return fail(PPF_ERR_INVALID, "n1m and n2m must be even (got %d, %d)", d->n1m, d->n2m);
+    if (!(d->L1 > 0.0) || !(d->L2 > 0.0)) return fail(PPF_ERR_INVALID, "L1, L2 must be positive");
+    if (d->precision < PPF_FP64 || d->precision > PPF_FP32)
+        return fail(PPF_ERR_INVALID, "unknown precision %d", d->precision);
+    if (d->max_sweeps > 8) return fail(PPF_ERR_INVALID, "max_sweeps %d > 8", d->max_sweeps);
+    if (d->n3m > 1024) return fail(PPF_ERR_UNSUPPORTED, "n3m %d > 1024", d->n3m);
+    FftSched s;
+    if (!factor(d->n1m / 2, s)) return fail(PPF_ERR_UNSUPPORTED, "n1m/2 = %d is not a product of 2, 3, 5", d->n1m / 2);
+    if (!factor(d->n2m, s)) return fail(PPF_ERR_UNSUPPORTED, "n2m = %d is not a product of 2, 3, 5", d->n2m);
+    const int limx = (d->precision == PPF_FP64) ? 2048 : 1024;
+    if (d->n1m > limx || d->n2m > 2048)
+        return fail(PPF_ERR_UNSUPPORTED, "n1m %d / n2m %d beyond the transform tile limits", d->n1m, d->n2m);
+    return PPF_OK;
+}
+
+long round_up(long v, long m) { return (v + m - 1) / m * m; }
+
+int plan_init(ppf_plan* p, const ppf_desc* d)
+{
+    p->d = *d;
+    if (p->d.max_sweeps < 0) p->d.max_sweeps = 2;
+    if (!(p->d.lowk_threshold > 0.0)) p->d.lowk_threshold = 1e-3;
+    PPF_CK(cudaGetDevice(&p->dev));
+    const int nx = d->n1m, ny = d->n2m, nz = d->n3m;
+    p->g.nx = nx; p->g.ny = ny; p->g.nz = nz;
+    p->g.px = d->pbc1 ? 1 : 0; p->g.py = d->pbc2 ? 1 : 0; p->g.pz = d->pbc3 ? 1 : 0;
+    p->g.pstride_y = nx + 2;
+    p->g.pstride_z = (long)(nx + 2) * (ny + 2);
+    p->xdct = !d->pbc1;
+    p->ydct = !d->pbc2;
+    p->elem = (d->precision == PPF_FP64) ? 8 : 4;
+    const size_t ce = 2 * p->elem;  // complex element bytes
+    factor(nx / 2, p->sx);
+    factor(ny, p->sy);
+
+    const int nh = nx / 2 + 1;
+    if (!p->xdct) {
+        // A: complex rows of nx/2+1
+        p->a_pitch = round_up(nh, 16);
+        p->a_bytes = (size_t)p->a_pitch * ny * nz * ce;
+        p->ycols = nh;
+        p->b_pitch = p->a_pitch;
+        p->ykind = p->ydct ? Y_CDCT : Y_C2C;
+        p->mx = nh; p->my = ny;
+        p->b_bytes = (size_t)p->b_pitch * ny * nz * ce;
+        p->cplx = true;
+    } else {
+        // A: real rows of nx (packed as nx/2 complex pairs in the y pass)
+        p->a_pitch = round_up(nx, 32);
+        p->a_bytes = (size_t)p->a_pitch * ny * nz * p->elem;
+        p->ycols = nx / 2;
+        if (p->ydct) {
+            p->ykind = Y_CDCT;
+            p->b_pitch = p->a_pitch;  // real
+            p->mx = nx; p->my = ny;
+            p->b_bytes = (size_t)p->b_pitch * ny * nz * p->elem;
+            p->cplx = false;
+        } else {
+            p->ykind = Y_RPAIR;
+            p->b_pitch = round_up(nx, 16);  // complex, ny/2+1 rows
+            p->mx = nx; p->my = ny / 2 + 1;
+            p->b_bytes = (size_t)p->b_pitch * (ny / 2 + 1) * nz * ce;
+            p->cplx = true;
+        }
+    }
+    // normalisation of the unnormalised inverse transforms: 1/n (FFT), 1/(2n) (DCT)
+    p->scale = 1.0 / ((p->xdct ? 2.0 * nx : (double)nx) * (p->ydct ? 2.0 * ny : (double)ny));
+
+    // eigenvalue tables (host FP64, the reference's formulas)
+    const double hx = d->L1 / nx, hy = d->L2 / ny;
+    std::vector<double> lx(p->mx), ly(p->my);
+    for (int i = 0; i < p->mx; ++i) lx[i] = p->xdct ? wn_dct(i, nx, hx) : wn_fft(i, nx, hx);
+    for (int j = 0; j < p->my; ++j) {
+        if (p->ydct) { ly[j] = wn_dct(j, ny, hy); continue; }
+        int jm = j;
+        if (!p->xdct && j + 1 > ny / 2 + 1) jm = ny - j;   // periodic-periodic fold (:339-346)
+        ly[j] = wn_fft(jm, ny, hy);
+    }
+    if (cudaMalloc(&p->A, p->a_bytes) != cudaSuccess || cudaMalloc(&p->B, p->b_bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(PPF_ERR_NOMEM, "cannot allocate %.1f MB of spectral work memory",
+                    (p->a_bytes + p->b_bytes) / 1048576.0);
+    }
+    PPF_CK(cudaMalloc(&p->lamx, sizeof(double) * p->mx));
+    PPF_CK(cudaMalloc(&p->lamy, sizeof(double) * p->my));
+    PPF_CK(cudaMalloc(&p->am, sizeof(double) * nz));
+    PPF_CK(cudaMalloc(&p->ap, sizeof(double) * nz));
+    PPF_CK(cudaMalloc(&p->scal, sizeof(double) * 4));
+    PPF_CK(cudaMalloc(&p->flags, sizeof(int) * 4));
+    PPF_CK(cudaMemset(p->scal, 0, sizeof(double) * 4));
+    PPF_CK(cudaMemset(p->flags, 0, sizeof(int) * 4));
+    PPF_CK(cudaMemcpy(p->lamx, lx.data(), sizeof(double) * p->mx, cudaMemcpyHostToDevice));
+    PPF_CK(cudaMemcpy(p->lamy, ly.data(), sizeof(double) * p->my, cudaMemcpyHostToDevice));
+    int rc = (p->elem == 8) ? upload_twiddles<double>(p) : upload_twiddles<float>(p);
+    return rc;
+}
+
+template <typename T>
+int run_pass(ppf_plan* p, const double* f, double* P, bool resid, bool accumulate, const int* skip,
+             cudaStream_t st)
+{
+    const cx<T>* tw = reinterpret_cast<const cx<T>*>(p->tw);
+    const cx<T>* txh = tw + p->tw_off[0];
+    const cx<T>* txn = tw + p->tw_off[1];
+    const cx<T>* txd = tw + p->tw_off[2];
+    const cx<T>* tyn = tw + p->tw_off[3];
+    const cx<T>* tyd = tw + p->tw_off[4];
+    ResidIn rs{};
+    if (resid) {
+        rs.P = P;
+        rs.am = p->am;
+        rs.ap = p->ap;
+        const double hx = p->d.L1 / p->g.nx, hy = p->d.L2 / p->g.ny;
+        rs.ix2 = 1.0 / (hx * hx);
+        rs.iy2 = 1.0 / (hy * hy);
+    }
+    cudaError_t e;
+    e = launch_xfwd<T>(p->xdct, f, resid ? &rs : nullptr, p->g, p->A, p->a_pitch, p->sx, txh, txn, txd, skip, st);
+    if (e != cudaSuccess) return cuda_fail(e, "x forward");
+    mark(p, 1, st);
+    // complex views of A and B for the y pass
+    const long a_cp = p->xdct ? p->a_pitch / 2 : p->a_pitch;
+    const long b_cp = (p->xdct && p->ydct) ? p->b_pitch / 2 : p->b_pitch;
+    e = launch_yfwd<T>(p->ykind, reinterpret_cast<const cx<T>*>(p->A), a_cp, reinterpret_cast<cx<T>*>(p->B), b_cp,
+                       p->ycols, p->g, p->sy, tyn, tyd, skip, st);
+    if (e != cudaSuccess) return cuda_fail(e, "y forward");
+    mark(p, 2, st);
+    ZSys z{};
+    z.mx = p->mx; z.my = p->my; z.pitch = p->b_pitch; z.plane = p->b_pitch * (long)p->my; z.nz = p->g.nz;
+    z.lamx = p->lamx; z.lamy = p->lamy; z.am = p->am; z.ap = p->ap; z.scale = p->scale;
+    z.lowk = (p->d.precision == PPF_FP64) ? 0.0 : p->d.lowk_threshold;
+    z.dzmax2 = p->scal;
+    e = p->cplx ? launch_tdma_z<T, true>(p->B, z, skip, p->flags + 2, st)
+                : launch_tdma_z<T, false>(p->B, z, skip, p->flags + 2, st);
+    if (e != cudaSuccess) return cuda_fail(e, "z tridiagonal");
+    mark(p, 3, st);
+    e = launch_yinv<T>(p->ykind, reinterpret_cast<const cx<T>*>(p->B), b_cp, reinterpret_cast<cx<T>*>(p->A), a_cp,
+                       p->ycols, p->g, p->sy, tyn, tyd, skip, st);
+    if (e != cudaSuccess) return cuda_fail(e, "y inverse");
+    mark(p, 4, st);
+    e = launch_xinv<T>(p->xdct, p->A, p->a_pitch, P, p->g, accumulate, accumulate ? p->scal + 1 : nullptr, p->sx,
+                       txh, txn, txd, skip, st);
+    if (e != cudaSuccess) return cuda_fail(e, "x inverse");
+    mark(p, 5, st);
+    return PPF_OK;
+}
+
+int solve_impl(ppf_plan* p, const double* f, double* P, const double* dmx1, const double* dmx2,
+               const double* dmx3, const double* dx3, cudaStream_t st)
+{
+    if (!p) return fail(PPF_ERR_INVALID, "null plan");
+    if (!f || !P || !dmx1 || !dmx2 || !dmx3 || !dx3) return fail(PPF_ERR_INVALID, "null array argument");
+    int cur = -1;
+    PPF_CK(cudaGetDevice(&cur));
+    if (cur != p->dev) return fail(PPF_ERR_STATE, "plan was created on device %d, current device is %d", p->dev, cur);
+    mark(p, -1, st);
+    PPF_CK(cudaMemsetAsync(p->flags, 0, sizeof(int) * 4, st));
+    PPF_CK(cudaMemsetAsync(p->scal + 1, 0, sizeof(double) * 3, st));
+    cudaError_t e = launch_zcoef(dx3, dmx3, p->g.nz, p->am, p->ap, p->scal, st);
+    if (e != cudaSuccess) return cuda_fail(e, "z coefficients");
+    mark(p, 0, st);
+    int rc;
+    if (p->elem == 8) {
+        rc = run_pass<double>(p, f, P, false, false, nullptr, st);
+    } else {
+        rc = run_pass<float>(p, f, P, false, false, nullptr, st);
+        if (rc == PPF_OK && p->d.precision == PPF_MIXED) {
+            for (int s = 0; s < p->d.max_sweeps && rc == PPF_OK; ++s) {
+                rc = run_pass<float>(p, f, P, true, true, p->flags, st);
+                if (rc != PPF_OK) break;
+                e = launch_sweep_gate(p->scal + 1, p->flags, p->flags + 1, p->scal + 3, p->d.sweep_tol, st);
+                if (e != cudaSuccess) return cuda_fail(e, "sweep gate");
+                mark(p, 6, st);
+            }
+        }
+    }
+    if (rc != PPF_OK) return rc;
+    e = launch_ghosts(P, p->g, dmx1, dmx2, dmx3, st);
+    if (e != cudaSuccess) return cuda_fail(e, "ghost cells");
+    mark(p, 7, st);
+    return PPF_OK;
+}
+
+// one module-global plan for the reference-shaped API (p_poi, fft_3d_poisson.f90:43-59)
+std::mutex g_mod_mu;
+ppf_desc g_mod_desc{};
+bool g_mod_desc_set = false;
+ppf_plan* g_mod_plan = nullptr;
+int g_mod_prec = PPF_FP64, g_mod_sweeps = -1;
+
+}  // namespace
+
+extern "C" {
+
+const char* ppf_last_error(void) { return g_err; }
+
+const char* ppf_version(void) { return "ppf 0.1.0 (sm_100a)"; }
+
+int ppf_plan_create(const ppf_desc* desc, ppf_plan** plan)
+{
+    g_err[0] = 0;
+    if (!plan) return fail(PPF_ERR_INVALID, "null plan pointer");
+    *plan = nullptr;
+    int rc = validate(desc);
+    if (rc != PPF_OK) return rc;
+    ppf_plan* p = new (std::nothrow) ppf_plan();
+    if (!p) return fail(PPF_ERR_NOMEM, "host allocation failed");
+    rc = plan_init(p, desc);
+    if (rc != PPF_OK) {
+        free_plan(p);
+        return rc;
+    }
+    *plan = p;
+    return PPF_OK;
+}
+
+int ppf_plan_destroy(ppf_plan* plan)
+{
+    free_plan(plan);
+    return PPF_OK;
+}
+
+int ppf_stage_timing(ppf_plan* plan, int enable)
+{
+    if (!plan) return fail(PPF_ERR_INVALID, "null plan");
+    plan->timing = enable != 0;
+    if (!plan->timing) drop_marks(plan);
+    return PPF_OK;
+}
+
+int ppf_stage_times(ppf_plan* plan, double* ms, int* launches)
+{
+    if (!plan || !ms || !launches) return fail(PPF_ERR_INVALID, "null argument");
+    for (int i = 0; i < PPF_NSTAGES; ++i) { ms[i] = 0.0; launches[i] = 0; }
+    cudaEvent_t prev = nullptr;
+    for (auto& m : plan->marks) {
+        cudaError_t e = cudaEventSynchronize(m.second);
+        if (e != cudaSuccess) { drop_marks(plan); return cuda_fail(e, "event synchronise"); }
+        if (m.first >= 0 && prev) {
+            float t = 0.f;
+            cudaEventElapsedTime(&t, prev, m.second);
+            ms[m.first] += t;
+            // ghosts launch one kernel per axis; every other stage one kernel
+            launches[m.first] += (m.first == 7) ? 3 : 1;
+        }
+        prev = m.second;
+    }
+    drop_marks(plan);
+    return PPF_OK;
+}
+
+int ppf_plan_workspace_bytes(const ppf_plan* plan, long long* bytes)
+{
+    if (!plan || !bytes) return fail(PPF_ERR_INVALID, "null argument");
+    *bytes = (long long)(plan->a_bytes + plan->b_bytes);
+    return PPF_OK;
+}
+
+int ppf_solve(ppf_plan* plan, const double* f_d, double* p_d, const double* dmx1_d, const double* dmx2_d,
+              const double* dmx3_d, const double* dx3_d, void* stream)
+{
+    g_err[0] = 0;
+    return solve_impl(plan, f_d, p_d, dmx1_d, dmx2_d, dmx3_d, dx3_d, (cudaStream_t)stream);
+}
+
+int ppf_solve_host(ppf_plan* plan, const double* f_h, double* p_h, const double* dmx1_h, const double* dmx2_h,
+                   const double* dmx3_h, const double* dx3_h, void* stream)
+{
+    g_err[0] = 0;
+    if (!plan) return fail(PPF_ERR_INVALID, "null plan");
+    if (!f_h || !p_h || !dmx1_h || !dmx2_h || !dmx3_h || !dx3_h) return fail(PPF_ERR_INVALID, "null array argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    const Geom& g = plan->g;
+    const size_t nf = (size_t)g.nx * g.ny * g.nz, np = (size_t)(g.nx + 2) * (g.ny + 2) * (g.nz + 2);
+    const size_t nm = (size_t)(g.nx + 2) + (g.ny + 2) + 2 * (g.nz + 2);
+    if (!plan->f_dev) {
+        if (cudaMalloc((void**)&plan->f_dev, nf * sizeof(double)) != cudaSuccess ||
+            cudaMalloc((void**)&plan->p_dev, np * sizeof(double)) != cudaSuccess ||
+            cudaMalloc((void**)&plan->m_dev, nm * sizeof(double)) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(PPF_ERR_NOMEM, "cannot allocate device staging for host arrays");
+        }
+    }
+    double *fd = plan->f_dev, *pd = plan->p_dev;
+    double* d1 = plan->m_dev;
+    double* d2 = d1 + (g.nx + 2);
+    double* d3 = d2 + (g.ny + 2);
+    double* x3 = d3 + (g.nz + 2);
+    PPF_CK(cudaMemcpyAsync(fd, f_h, nf * sizeof(double), cudaMemcpyHostToDevice, st));
+    PPF_CK(cudaMemcpyAsync(d1, dmx1_h, (g.nx + 2) * sizeof(double), cudaMemcpyHostToDevice, st));
+    PPF_CK(cudaMemcpyAsync(d2, dmx2_h, (g.ny + 2) * sizeof(double), cudaMemcpyHostToDevice, st));
+    PPF_CK(cudaMemcpyAsync(d3, dmx3_h, (g.nz + 2) * sizeof(double), cudaMemcpyHostToDevice, st));
+    PPF_CK(cudaMemcpyAsync(x3, dx3_h, (g.nz + 2) * sizeof(double), cudaMemcpyHostToDevice, st));
+    int rc = solve_impl(plan, fd, pd, d1, d2, d3, x3, st);
+    if (rc == PPF_OK) {
+        cudaError_t e = cudaMemcpyAsync(p_h, pd, np * sizeof(double), cudaMemcpyDeviceToHost, st);
+        if (e != cudaSuccess) rc = cuda_fail(e, "copy out");
+    }
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (rc == PPF_OK && e != cudaSuccess) rc = cuda_fail(e, "synchronise");
+    return rc;
+}
+
+int ppf_last_sweeps(ppf_plan* plan, int* sweeps, double* last_rel_update, void* stream)
+{
+    if (!plan) return fail(PPF_ERR_INVALID, "null plan");
+    int fl[4];
+    double sc[4];
+    cudaStream_t st = (cudaStream_t)stream;
+    PPF_CK(cudaMemcpyAsync(fl, plan->flags, sizeof(fl), cudaMemcpyDeviceToHost, st));
+    PPF_CK(cudaMemcpyAsync(sc, plan->scal, sizeof(sc), cudaMemcpyDeviceToHost, st));
+    PPF_CK(cudaStreamSynchronize(st));
+    if (sweeps) *sweeps = fl[1];
+    if (last_rel_update) *last_rel_update = sc[3];
+    if (fl[2]) return fail(PPF_ERR_NUMERIC, "a tridiagonal solve produced a non-finite value");
+    return PPF_OK;
+}
+
+// ---- reference-shaped API -------------------------------------------------
+
+int ppf_fft_poisson_plan_cuda_create(int n1, int n2, int n3, double L1, double L2, double L3, int pbc1, int pbc2,
+                                     int pbc3)
+{
+    g_err[0] = 0;
+    (void)L3;
+    std::lock_guard<std::mutex> lk(g_mod_mu);
+    ppf_desc d{};
+    d.n1m = n1 - 1; d.n2m = n2 - 1; d.n3m = n3 - 1;     // n*m = n* - 1 (:103-104)
+    d.L1 = L1; d.L2 = L2;
+    d.pbc1 = pbc1 ? 1 : 0; d.pbc2 = pbc2 ? 1 : 0; d.pbc3 = pbc3 ? 1 : 0;
+    d.precision = g_mod_prec;
+    d.max_sweeps = g_mod_sweeps;
+    int rc = validate(&d);
+    if (rc != PPF_OK) return rc;
+    g_mod_desc = d;
+    g_mod_desc_set = true;
+    return PPF_OK;
+}
+
+int ppf_cuda_poisson_fft_set_precision(int precision, int max_sweeps)
+{
+    std::lock_guard<std::mutex> lk(g_mod_mu);
+    if (precision < PPF_FP64 || precision > PPF_FP32) return fail(PPF_ERR_INVALID, "unknown precision %d", precision);
+    g_mod_prec = precision;
+    g_mod_sweeps = max_sweeps;
+    return PPF_OK;
+}
+
+int ppf_cuda_poisson_fft_initial(void)
+{
+    g_err[0] = 0;
+    std::lock_guard<std::mutex> lk(g_mod_mu);
+    if (!g_mod_desc_set) return fail(PPF_ERR_STATE, "ppf_fft_poisson_plan_cuda_create was not called");
+    if (g_mod_plan) { free_plan(g_mod_plan); g_mod_plan = nullptr; }
+    ppf_desc d = g_mod_desc;
+    d.precision = g_mod_prec;
+    d.max_sweeps = g_mod_sweeps;
+    return ppf_plan_create(&d, &g_mod_plan);
+}
+
+int ppf_cuda_poisson_fft_1d(double* PRHS_d, double* P_d, const double* dmx1_d, const double* dmx2_d,
+                            const double* dmx3_d, const double* dx3_d)
+{
+    g_err[0] = 0;
+    std::lock_guard<std::mutex> lk(g_mod_mu);
+    if (!g_mod_plan) return fail(PPF_ERR_STATE, "ppf_cuda_poisson_fft_initial was not called");
+    int rc = solve_impl(g_mod_plan, PRHS_d, P_d, dmx1_d, dmx2_d, dmx3_d, dx3_d, (cudaStream_t)0);
+    if (rc != PPF_OK) return rc;
+    // the reference call is synchronous on the default stream
+    cudaError_t e = cudaStreamSynchronize((cudaStream_t)0);
+    if (e != cudaSuccess) return cuda_fail(e, "synchronise");
+    return PPF_OK;
+}
+
+int ppf_cuda_poisson_fft_clean(void)
+{
+    std::lock_guard<std::mutex> lk(g_mod_mu);
+    free_plan(g_mod_plan);
+    g_mod_plan = nullptr;
+    g_mod_desc_set = false;
+    return PPF_OK;
+}
+
+// ---- batched tridiagonal solves on coefficient arrays ----------------------
+
+int ppf_tdma_many(const double* a, const double* b, const double* c, double* d, int n_sys, int n_row, void* stream)
+{
+    g_err[0] = 0;
+    if (!a || !b || !c || !d) return fail(PPF_ERR_INVALID, "null array argument");
+    if (n_sys < 1 || n_row < 1) return fail(PPF_ERR_INVALID, "n_sys %d, n_row %d must be positive", n_sys, n_row);
+    if (n_row > 1024) return fail(PPF_ERR_UNSUPPORTED, "n_row %d > 1024", n_row);
+    cudaError_t e = launch_tdma_many(a, b, c, d, n_sys, n_row, false, nullptr, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "tdma_many");
+    return PPF_OK;
+}
+
+int ppf_tdma_cycl_many(const double* a, const double* b, const double* c, double* d, int n_sys, int n_row,
+                       void* stream)
+{
+    g_err[0] = 0;
+    if (!a || !b || !c || !d) return fail(PPF_ERR_INVALID, "null array argument");
+    if (n_sys < 1 || n_row < 3) return fail(PPF_ERR_INVALID, "n_sys %d must be >= 1 and n_row %d >= 3", n_sys, n_row);
+    if (n_row > 1025) return fail(PPF_ERR_UNSUPPORTED, "n_row %d > 1025", n_row);
+    cudaError_t e = launch_tdma_many(a, b, c, d, n_sys, n_row, true, nullptr, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "tdma_cycl_many");
+    return PPF_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,224 @@
+// ppf_fft.cuh -- shared-memory Stockham FFT engine of libppf (sm_100a).
+//
+// A CTA holds W interleaved complex lines of length n in shared memory
+// (layout of sidx()).  Each pass of radix R computes all n/R butterflies of
+// all W lines: every thread first loads the inputs of its butterflies into
+// registers, the CTA synchronises, then the butterflies are applied and the
+// outputs stored in Stockham autosort order, so the tile is transformed in
+// place and ends in natural order.  Forward uses e^{-2 pi i jk/n}, inverse
+// e^{+2 pi i jk/n}; neither normalises (the reference's cuFFT/FFTW
+// convention, fft_3d_poisson.f90:195-286).
+#pragma once
+#include "ppf_common.cuh"
+
+namespace ppf {
+
+template <typename T> struct K;
+template <> struct K<double> {
+    static constexpr double s3 = 0.86602540378443864676;   // sin(pi/3)
+    static constexpr double r2 = 0.70710678118654752440;   // 1/sqrt(2)
+    static constexpr double c1 = 0.30901699437494742410;   // cos(2pi/5)
+    static constexpr double c2 = -0.80901699437494742410;  // cos(4pi/5)
+    static constexpr double s1 = 0.95105651629515357212;   // sin(2pi/5)
+    static constexpr double s2 = 0.58778525229247312917;   // sin(4pi/5)
+    static constexpr double c16 = 0.92387953251128675613;  // cos(pi/8)
+    static constexpr double s16 = 0.38268343236508977173;  // sin(pi/8)
+};
+template <> struct K<float> {
+    static constexpr float s3 = 0.86602540378443864676f;
+    static constexpr float r2 = 0.70710678118654752440f;
+    static constexpr float c1 = 0.30901699437494742410f;
+    static constexpr float c2 = -0.80901699437494742410f;
+    static constexpr float s1 = 0.95105651629515357212f;
+    static constexpr float s2 = 0.58778525229247312917f;
+    static constexpr float c16 = 0.92387953251128675613f;
+    static constexpr float s16 = 0.38268343236508977173f;
+};
+
+template <typename T, bool INV, int R> struct Dft;
+
+template <typename T, bool INV> struct Dft<T, INV, 2> {
+    static __device__ __forceinline__ void run(cx<T>* v)
+    {
+        cx<T> a = v[0], b = v[1];
+        v[0] = a + b;
+        v[1] = a - b;
+    }
+};
+
+template <typename T, bool INV> struct Dft<T, INV, 4> {
+    static __device__ __forceinline__ void run(cx<T>* v)
+    {
+        cx<T> a0 = v[0] + v[2], a1 = v[0] - v[2];
+        cx<T> b0 = v[1] + v[3], b1 = mul_mi<T, INV>(v[1] - v[3]);
+        v[0] = a0 + b0;
+        v[2] = a0 - b0;
+        v[1] = a1 + b1;
+        v[3] = a1 - b1;
+    }
+};
+
+template <typename T, bool INV> struct Dft<T, INV, 3> {
+    static __device__ __forceinline__ void run(cx<T>* v)
+    {
+        cx<T> t1 = v[1] + v[2];
+        cx<T> t2 = v[0] - t1 * (T)0.5;
+        // forward: (-i sin(pi/3)) (x1 - x2); inverse: (+i sin(pi/3)) (x1 - x2)
+        cx<T> t3 = mul_mi<T, INV>(v[1] - v[2]) * K<T>::s3;
+        v[0] = v[0] + t1;
+        v[1] = t2 + t3;
+        v[2] = t2 - t3;
+    }
+};
+
+template <typename T, bool INV> struct Dft<T, INV, 5> {
+    static __device__ __forceinline__ void run(cx<T>* v)
+    {
+        cx<T> t1 = v[1] + v[4], t2 = v[2] + v[3];
+        cx<T> t3 = v[1] - v[4], t4 = v[2] - v[3];
+        cx<T> a1 = v[0] + t1 * K<T>::c1 + t2 * K<T>::c2;
+        cx<T> a2 = v[0] + t1 * K<T>::c2 + t2 * K<T>::c1;
+        cx<T> b1 = t3 * K<T>::s1 + t4 * K<T>::s2;
+        cx<T> b2 = t3 * K<T>::s2 - t4 * K<T>::s1;
+        // forward: y1 = a1 - i b1, y4 = a1 + i b1, y2 = a2 - i b2, y3 = a2 + i b2
+        cx<T> mb1 = mul_mi<T, INV>(b1), mb2 = mul_mi<T, INV>(b2);
+        v[0] = v[0] + t1 + t2;
+        v[1] = a1 + mb1;
+        v[4] = a1 - mb1;
+        v[2] = a2 + mb2;
+        v[3] = a2 - mb2;
+    }
+};
+
+// w8^k multipliers for k = 1,2,3 (forward w8 = e^{-i pi/4})
+template <typename T, bool INV>
+__device__ __forceinline__ cx<T> w8(cx<T> a, int k)
+{
+    const T r = K<T>::r2;
+    if (k == 1) return INV ? mk((a.x - a.y) * r, (a.x + a.y) * r) : mk((a.x + a.y) * r, (a.y - a.x) * r);
+    if (k == 2) return mul_mi<T, INV>(a);
+    return INV ? mk(-(a.x + a.y) * r, (a.x - a.y) * r) : mk((a.y - a.x) * r, -(a.x + a.y) * r);
+}
+
+template <typename T, bool INV> struct Dft<T, INV, 8> {
+    static __device__ __forceinline__ void run(cx<T>* v)
+    {
+        cx<T> a[4], b[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            a[k] = v[k] + v[k + 4];
+            b[k] = v[k] - v[k + 4];
+        }
+        b[1] = w8<T, INV>(b[1], 1);
+        b[2] = w8<T, INV>(b[2], 2);
+        b[3] = w8<T, INV>(b[3], 3);
+        Dft<T, INV, 4>::run(a);
+        Dft<T, INV, 4>::run(b);
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            v[2 * m] = a[m];
+            v[2 * m + 1] = b[m];
+        }
+    }
+};
+
+template <typename T, bool INV> struct Dft<T, INV, 16> {
+    static __device__ __forceinline__ void run(cx<T>* v)
+    {
+        cx<T> a[8], b[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            a[k] = v[k] + v[k + 8];
+            b[k] = v[k] - v[k + 8];
+        }
+        // b[k] *= w16^k, w16 = e^{-i pi/8} (forward)
+        const T c = K<T>::c16, s = K<T>::s16, r = K<T>::r2;
+        const T sg = INV ? (T)1 : (T)-1;
+        const cx<T> w1 = mk(c, sg * s), w3 = mk(s, sg * c), w5 = mk(-s, sg * c), w7 = mk(-c, sg * s);
+        b[1] = cmul(b[1], w1);
+        b[2] = w8<T, INV>(b[2], 1);
+        b[3] = cmul(b[3], w3);
+        b[4] = mul_mi<T, INV>(b[4]);
+        b[5] = cmul(b[5], w5);
+        b[6] = w8<T, INV>(b[6], 3);
+        b[7] = cmul(b[7], w7);
+        (void)r;
+        Dft<T, INV, 8>::run(a);
+        Dft<T, INV, 8>::run(b);
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+            v[2 * m] = a[m];
+            v[2 * m + 1] = b[m];
+        }
+    }
+};
+
+// One Stockham pass of radix R over the W-line tile.  tw[k] = e^{-2 pi i k/n}.
+// v is the caller's register buffer (VMAX complex), shared by every radix so
+// that all passes reuse the same registers.
+constexpr int VMAX = 10;
+
+template <typename T, bool INV, int R>
+__device__ __forceinline__ void fft_pass(cx<T>* s, int n, int W, int lgW, int Ns, const cx<T>* __restrict__ tw,
+                                         cx<T> (&v)[VMAX])
+{
+    constexpr int Q = (8 + R - 1) / R;  // butterflies per thread: tiles launch >= n*W/8 threads
+    static_assert(Q * R <= VMAX, "register buffer too small");
+    const int nb = n / R;
+    const int items = nb << lgW;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        const int t = threadIdx.x + q * blockDim.x;
+        if (t < items) {
+            const int l = t & (W - 1), j = t >> lgW;
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[q * R + r] = s[sidx<T>(j + r * nb, l, W)];
+        }
+    }
+    __syncthreads();
+    const int tstride = n / (Ns * R);
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        const int t = threadIdx.x + q * blockDim.x;
+        if (t < items) {
+            const int l = t & (W - 1), j = t >> lgW;
+            const int k = j % Ns;
+            if (Ns > 1) {
+#pragma unroll
+                for (int r = 1; r < R; ++r) {
+                    cx<T> w = ldg(tw + r * k * tstride);
+                    if (INV) w.y = -w.y;
+                    v[q * R + r] = cmul(v[q * R + r], w);
+                }
+            }
+            Dft<T, INV, R>::run(v + q * R);
+            const int base = (j - k) * R + k;
+#pragma unroll
+            for (int r = 0; r < R; ++r) s[sidx<T>(base + r * Ns, l, W)] = v[q * R + r];
+        }
+    }
+    __syncthreads();
+}
+
+// Full transform of the tile.  Caller synchronises before (tile loaded);
+// the tile is complete and visible to all threads on return.
+template <typename T, bool INV>
+__device__ __forceinline__ void fft_tile(cx<T>* s, const FftSched& sch, int W, int lgW,
+                                         const cx<T>* __restrict__ tw)
+{
+    cx<T> v[VMAX];
+    int Ns = 1;
+    for (int p = 0; p < sch.npass; ++p) {
+        const int R = sch.radix[p];
+        switch (R) {
+            case 2: fft_pass<T, INV, 2>(s, sch.n, W, lgW, Ns, tw, v); break;
+            case 3: fft_pass<T, INV, 3>(s, sch.n, W, lgW, Ns, tw, v); break;
+            case 4: fft_pass<T, INV, 4>(s, sch.n, W, lgW, Ns, tw, v); break;
+            case 5: fft_pass<T, INV, 5>(s, sch.n, W, lgW, Ns, tw, v); break;
+            default: fft_pass<T, INV, 8>(s, sch.n, W, lgW, Ns, tw, v); break;
+        }
+        Ns *= R;
+    }
+}
+
+}  // namespace ppf

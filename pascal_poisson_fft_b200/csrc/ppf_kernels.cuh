@@ -1,0 +1,87 @@
+// ppf_kernels.cuh -- launch interfaces of the libppf kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include "ppf_common.cuh"
+
+namespace ppf {
+
+// Geometry of a solve, as the kernels see it.
+struct Geom {
+    int nx, ny, nz;       // cells
+    int px, py, pz;       // periodic flags
+    long pstride_y;       // ghosted P strides (elements): (nx+2)
+    long pstride_z;       // (nx+2)*(ny+2)
+};
+
+// Residual-input options of the x-forward pass (FP64 residual refinement).
+struct ResidIn {
+    const double* P;      // current iterate, ghosted layout (interior read)
+    const double* am;     // z coefficient tables (nz)
+    const double* ap;
+    double ix2, iy2;      // 1/dx^2, 1/dy^2 (uniform x, y)
+};
+
+// Accumulation options of the x-inverse pass.
+struct AccumOut {
+    double* norms;        // [0] += sum du^2, [1] += sum u_new^2 (may be null)
+};
+
+enum YKind { Y_C2C = 0, Y_CDCT = 1, Y_RPAIR = 2 };
+
+// ---- launchers (defined in ppf_xy.cu) ----
+template <typename T>
+cudaError_t launch_xfwd(bool dct, const double* f, const ResidIn* resid, const Geom& g,
+                        void* out, long out_pitch, const FftSched& sch,
+                        const cx<T>* tw_half, const cx<T>* tw_n, const cx<T>* tw_dct,
+                        const int* skip_flag, cudaStream_t st);
+
+template <typename T>
+cudaError_t launch_yfwd(int kind, const cx<T>* in, long in_pitch, cx<T>* out, long out_pitch,
+                        int ncols, const Geom& g, const FftSched& sch,
+                        const cx<T>* tw_ny, const cx<T>* tw_dct, const int* skip_flag, cudaStream_t st);
+
+template <typename T>
+cudaError_t launch_yinv(int kind, const cx<T>* in, long in_pitch, cx<T>* out, long out_pitch,
+                        int ncols, const Geom& g, const FftSched& sch,
+                        const cx<T>* tw_ny, const cx<T>* tw_dct, const int* skip_flag, cudaStream_t st);
+
+template <typename T>
+cudaError_t launch_xinv(bool dct, const void* in, long in_pitch, double* P, const Geom& g,
+                        bool accumulate, double* norms, const FftSched& sch,
+                        const cx<T>* tw_half, const cx<T>* tw_n, const cx<T>* tw_dct,
+                        const int* skip_flag, cudaStream_t st);
+
+// ---- Poisson TDMA along z (ppf_tdma.cu) ----
+struct ZSys {
+    int mx, my;           // system grid (kx < mx, ky < my)
+    long pitch;           // elements per spectral row (>= mx)
+    long plane;           // elements per z plane (pitch * my)
+    int nz;
+    const double* lamx;   // eigenvalue tables (mx), (my)
+    const double* lamy;
+    const double* am;     // z coefficient tables (nz)
+    const double* ap;
+    double scale;         // normalisation folded into the solution
+    double lowk;          // FP32 storage: systems with lam*dzmax^2 < lowk solve in FP64
+    const double* dzmax2; // device scalar: max_k dx3_k^2 (written by the z-coefficient kernel)
+};
+
+template <typename T, bool CPLX>
+cudaError_t launch_tdma_z(void* data, const ZSys& z, const int* skip_flag, int* err_flag, cudaStream_t st);
+
+cudaError_t launch_zcoef(const double* dx3, const double* dmx3, int nz, double* am, double* ap,
+                         double* dzmax2, cudaStream_t st);
+
+// ---- ghost cells (ppf_ghost.cu) ----
+cudaError_t launch_ghosts(double* P, const Geom& g, const double* dmx1, const double* dmx2,
+                          const double* dmx3, cudaStream_t st);
+
+// ---- generic batched TDMA on coefficient arrays (ppf_tdma.cu) ----
+cudaError_t launch_tdma_many(const double* a, const double* b, const double* c, double* d,
+                             int n_sys, int n_row, bool cyclic, int* err, cudaStream_t st);
+
+// refinement bookkeeping: decides whether the next sweep runs
+cudaError_t launch_sweep_gate(double* norms, int* skip_flag, int* sweeps_done, double* last_rel,
+                              double tol, cudaStream_t st);
+
+}  // namespace ppf

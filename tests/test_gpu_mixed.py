@@ -1,0 +1,46 @@
+"""Mixed precision (FP32 transforms + FP64 residual refinement) and FP32."""
+import numpy as np
+import pytest
+
+from _util import gpu_solve, oracle_solve, rel_l2
+from pascal_poisson_fft_b200 import PPF_FP32, PPF_MIXED
+from pascal_poisson_fft_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+TOL_MIXED = 1e-10   # mixed + refinement vs FP64, rel-L2
+TOL_FP32 = 5e-5     # a single FP32 solve vs FP64, rel-L2
+
+
+@pytest.mark.parametrize("pbc", [(1, 1, 0), (0, 0, 0), (0, 1, 0), (1, 0, 0)])
+def test_mixed_matches_oracle(pbc):
+    rng = np.random.default_rng(21)
+    p = W.random_problem(rng, 64, 48, 64, pbc, beta=1.5)
+    R = oracle_solve(p)
+    P = gpu_solve(p, precision=PPF_MIXED, max_sweeps=3)
+    assert rel_l2(P, R) < TOL_MIXED
+
+
+@pytest.mark.parametrize("pbc", [(1, 1, 0), (0, 0, 0)])
+def test_fp32_single_solve_accuracy(pbc):
+    rng = np.random.default_rng(22)
+    p = W.random_problem(rng, 64, 64, 64, pbc, beta=1.5)
+    R = oracle_solve(p)
+    P = gpu_solve(p, precision=PPF_FP32)
+    assert rel_l2(P, R) < TOL_FP32
+
+
+def test_mixed_config3_shape_256():
+    p = W.config3(n1m=256, n2m=256, n3m=256)
+    P64 = gpu_solve(p)
+    P = gpu_solve(p, precision=PPF_MIXED, max_sweeps=2)
+    assert rel_l2(P, P64) < TOL_MIXED
+
+
+def test_sweep_gate_stops_early():
+    rng = np.random.default_rng(23)
+    p = W.random_problem(rng, 64, 64, 64, (1, 1, 0), beta=1.5)
+    P, plan = gpu_solve(p, precision=PPF_MIXED, max_sweeps=6, sweep_tol=1e-9, return_plan=True)
+    sweeps, rel = plan.last_sweeps()
+    assert 1 <= sweeps < 6 and rel < 1e-9
+    R = oracle_solve(p)
+    assert rel_l2(P, R) < TOL_MIXED
