@@ -453,11 +453,12 @@ static void z_coeffs(int n3m, const double *dx3, const double *dmx3, double *am,
 }
 
 /* Solve one block of systems (system index fastest, nz rows) whose diagonal
- * shift is lam[s]; pin applies to system `pin_sys` (or none if < 0).
- * d is overwritten with the solution.  pbc3 selects the cyclic solver
- * (cuda_ptdma_core :898-913). */
+ * is ac - lx[s] - ly[s] (evaluated left to right, as
+ * `b = ac - dxk2(i) - dyk2(j)` at fft_3d_poisson.f90:1146, 1233, 1294);
+ * pin applies to system `pin_sys` (or none if < 0).  d is overwritten with
+ * the solution.  pbc3 selects the cyclic solver (cuda_ptdma_core :898-913). */
 static void solve_block(int nsys, int nz, const double *am, const double *ap,
-                        const double *lam, int pin_sys, int pbc3, double *d)
+                        const double *lx, const double *ly, int pin_sys, int pbc3, double *d)
 {
     size_t N = (size_t)nsys * nz;
     double *a = (double *)malloc(N * sizeof(double));
@@ -468,7 +469,7 @@ static void solve_block(int nsys, int nz, const double *am, const double *ap,
         for (int s = 0; s < nsys; ++s) {
             size_t id = (size_t)k * nsys + s;
             a[id] = am[k];
-            b[id] = ac - lam[s];
+            b[id] = ac - lx[s] - ly[s];
             c[id] = ap[k];
         }
     }
@@ -547,10 +548,10 @@ int ora_poisson_solve(int n1m, int n2m, int n3m, double L1, double L2,
             double *d = (double *)malloc(sizeof(double) * nx * nz);
             OMP_FOR
             for (long j = 0; j < ny; ++j) {
-                for (long i = 0; i < nx; ++i) lam[i] = dxk2[i] + dyk2[j];
+                for (long i = 0; i < nx; ++i) lam[i] = dyk2[j];
                 for (long k = 0; k < nz; ++k)
                     for (long i = 0; i < nx; ++i) d[k * nx + i] = X[k * nx * ny + j * nx + i];
-                solve_block((int)nx, (int)nz, am, ap, lam, j == 0 ? 0 : -1, pbc3, d);
+                solve_block((int)nx, (int)nz, am, ap, dxk2, lam, j == 0 ? 0 : -1, pbc3, d);
                 for (long k = 0; k < nz; ++k)
                     for (long i = 0; i < nx; ++i) X[k * nx * ny + j * nx + i] = d[k * nx + i];
             }
@@ -603,14 +604,14 @@ int ora_poisson_solve(int n1m, int n2m, int n3m, double L1, double L2,
             double *di = (double *)malloc(sizeof(double) * nx * nz);
             OMP_FOR
             for (long j = 0; j < hy; ++j) {                   /* :1276-1334 */
-                for (long i = 0; i < nx; ++i) lam[i] = dxk2[i] + dyk2[j];
+                for (long i = 0; i < nx; ++i) lam[i] = dyk2[j];
                 for (long k = 0; k < nz; ++k)
                     for (long i = 0; i < nx; ++i) {
                         cd v = C[k * nx * hy + j * nx + i];
                         dr[k * nx + i] = v.re; di[k * nx + i] = v.im;
                     }
-                solve_block((int)nx, (int)nz, am, ap, lam, j == 0 ? 0 : -1, pbc3, dr);
-                solve_block((int)nx, (int)nz, am, ap, lam, j == 0 ? 0 : -1, pbc3, di);
+                solve_block((int)nx, (int)nz, am, ap, dxk2, lam, j == 0 ? 0 : -1, pbc3, dr);
+                solve_block((int)nx, (int)nz, am, ap, dxk2, lam, j == 0 ? 0 : -1, pbc3, di);
                 for (long k = 0; k < nz; ++k)
                     for (long i = 0; i < nx; ++i) {
                         cd v = { dr[k * nx + i], di[k * nx + i] };
@@ -665,14 +666,14 @@ int ora_poisson_solve(int n1m, int n2m, int n3m, double L1, double L2,
             double *di = (double *)malloc(sizeof(double) * ny * nz);
             OMP_FOR
             for (long i = 0; i < hx; ++i) {                   /* :1215-1272, systems (j,i) */
-                for (long j = 0; j < ny; ++j) lam[j] = dxk2[i] + dyk2[j];
+                for (long j = 0; j < ny; ++j) lam[j] = dxk2[i];
                 for (long k = 0; k < nz; ++k)
                     for (long j = 0; j < ny; ++j) {
                         cd v = C[k * hx * ny + j * hx + i];
                         dr[k * ny + j] = v.re; di[k * ny + j] = v.im;
                     }
-                solve_block((int)ny, (int)nz, am, ap, lam, i == 0 ? 0 : -1, pbc3, dr);
-                solve_block((int)ny, (int)nz, am, ap, lam, i == 0 ? 0 : -1, pbc3, di);
+                solve_block((int)ny, (int)nz, am, ap, lam, dyk2, i == 0 ? 0 : -1, pbc3, dr);
+                solve_block((int)ny, (int)nz, am, ap, lam, dyk2, i == 0 ? 0 : -1, pbc3, di);
                 for (long k = 0; k < nz; ++k)
                     for (long j = 0; j < ny; ++j) {
                         cd v = { dr[k * ny + j], di[k * ny + j] };
@@ -726,14 +727,14 @@ int ora_poisson_solve(int n1m, int n2m, int n3m, double L1, double L2,
             double *di = (double *)malloc(sizeof(double) * ny * nz);
             OMP_FOR
             for (long i = 0; i < hx; ++i) {                   /* :1215-1272, systems (j,i) */
-                for (long j = 0; j < ny; ++j) lam[j] = dxk2[i] + dyk2[j];
+                for (long j = 0; j < ny; ++j) lam[j] = dxk2[i];
                 for (long k = 0; k < nz; ++k)
                     for (long j = 0; j < ny; ++j) {
                         cd v = C[k * hx * ny + j * hx + i];
                         dr[k * ny + j] = v.re; di[k * ny + j] = v.im;
                     }
-                solve_block((int)ny, (int)nz, am, ap, lam, i == 0 ? 0 : -1, pbc3, dr);
-                solve_block((int)ny, (int)nz, am, ap, lam, i == 0 ? 0 : -1, pbc3, di);
+                solve_block((int)ny, (int)nz, am, ap, lam, dyk2, i == 0 ? 0 : -1, pbc3, dr);
+                solve_block((int)ny, (int)nz, am, ap, lam, dyk2, i == 0 ? 0 : -1, pbc3, di);
                 if (cpu_fft1_imag_zero && i == 0) {
                     /* module_solve_poisson.f90:389-397 */
                     for (long k = 0; k < nz; ++k) { di[k * ny + 0] = 0.0; di[k * ny + ny / 2] = 0.0; }

@@ -103,8 +103,10 @@ struct ppf_plan {
     double* lamy = nullptr;
     double* am = nullptr;
     double* ap = nullptr;
-    double* scal = nullptr;    // [0] dzmax2, [1..2] norms, [3] last_rel
+    double* scal = nullptr;    // [0] dzmax2, [3] last ||du||/||u||, [4] zero-mode shift, [5] mean of the iterate
     int* flags = nullptr;      // [0] skip, [1] sweeps_done, [2] err
+    double* partials = nullptr;  // per-block sums of the x-inverse pass (mixed precision)
+    long xinv_nblk = 0;
     void* tw = nullptr;        // twiddle tables (type T)
     size_t tw_off[5] = {};     // element offsets: x half, x n, x dct, y n, y dct
     FftSched sx{}, sy{};
@@ -165,7 +167,7 @@ void free_plan(ppf_plan* p)
     if (!p) return;
     drop_marks(p);
     void* ptrs[] = { p->A, p->B, p->lamx, p->lamy, p->am, p->ap, p->scal, p->flags, p->tw,
-                     p->f_dev, p->p_dev, p->m_dev };
+                     p->f_dev, p->p_dev, p->m_dev, p->partials };
     for (void* q : ptrs)
         if (q) cudaFree(q);
     delete p;
@@ -264,10 +266,14 @@ int plan_init(ppf_plan* p, const ppf_desc* d)
     PPF_CK(cudaMalloc(&p->lamy, sizeof(double) * p->my));
     PPF_CK(cudaMalloc(&p->am, sizeof(double) * nz));
     PPF_CK(cudaMalloc(&p->ap, sizeof(double) * nz));
-    PPF_CK(cudaMalloc(&p->scal, sizeof(double) * 4));
+    PPF_CK(cudaMalloc(&p->scal, sizeof(double) * 8));
     PPF_CK(cudaMalloc(&p->flags, sizeof(int) * 4));
-    PPF_CK(cudaMemset(p->scal, 0, sizeof(double) * 4));
+    PPF_CK(cudaMemset(p->scal, 0, sizeof(double) * 8));
     PPF_CK(cudaMemset(p->flags, 0, sizeof(int) * 4));
+    if (p->d.precision == PPF_MIXED) {
+        p->xinv_nblk = xinv_blocks<float>(p->g);
+        PPF_CK(cudaMalloc(&p->partials, sizeof(double) * 3 * p->xinv_nblk));
+    }
     PPF_CK(cudaMemcpy(p->lamx, lx.data(), sizeof(double) * p->mx, cudaMemcpyHostToDevice));
     PPF_CK(cudaMemcpy(p->lamy, ly.data(), sizeof(double) * p->my, cudaMemcpyHostToDevice));
     int rc = (p->elem == 8) ? upload_twiddles<double>(p) : upload_twiddles<float>(p);
@@ -309,15 +315,17 @@ int run_pass(ppf_plan* p, const double* f, double* P, bool resid, bool accumulat
     z.lamx = p->lamx; z.lamy = p->lamy; z.am = p->am; z.ap = p->ap; z.scale = p->scale;
     z.lowk = (p->d.precision == PPF_FP64) ? 0.0 : p->d.lowk_threshold;
     z.dzmax2 = p->scal;
+    z.dc_shift = p->scal + 4;
+    z.cyclic = p->g.pz;
     e = p->cplx ? launch_tdma_z<T, true>(p->B, z, skip, p->flags + 2, st)
                 : launch_tdma_z<T, false>(p->B, z, skip, p->flags + 2, st);
     if (e != cudaSuccess) return cuda_fail(e, "z tridiagonal");
     mark(p, 3, st);
     e = launch_yinv<T>(p->ykind, reinterpret_cast<const cx<T>*>(p->B), b_cp, reinterpret_cast<cx<T>*>(p->A), a_cp,
-                       p->ycols, p->g, p->sy, tyn, tyd, skip, st);
+                       p->ycols, p->g, p->sy, tyn, tyd, p->scal + 4, skip, st);
     if (e != cudaSuccess) return cuda_fail(e, "y inverse");
     mark(p, 4, st);
-    e = launch_xinv<T>(p->xdct, p->A, p->a_pitch, P, p->g, accumulate, accumulate ? p->scal + 1 : nullptr, p->sx,
+    e = launch_xinv<T>(p->xdct, p->A, p->a_pitch, P, p->g, accumulate, p->partials, p->scal + 5, p->sx,
                        txh, txn, txd, skip, st);
     if (e != cudaSuccess) return cuda_fail(e, "x inverse");
     mark(p, 5, st);
@@ -334,7 +342,7 @@ int solve_impl(ppf_plan* p, const double* f, double* P, const double* dmx1, cons
     if (cur != p->dev) return fail(PPF_ERR_STATE, "plan was created on device %d, current device is %d", p->dev, cur);
     mark(p, -1, st);
     PPF_CK(cudaMemsetAsync(p->flags, 0, sizeof(int) * 4, st));
-    PPF_CK(cudaMemsetAsync(p->scal + 1, 0, sizeof(double) * 3, st));
+    PPF_CK(cudaMemsetAsync(p->scal + 1, 0, sizeof(double) * 7, st));
     cudaError_t e = launch_zcoef(dx3, dmx3, p->g.nz, p->am, p->ap, p->scal, st);
     if (e != cudaSuccess) return cuda_fail(e, "z coefficients");
     mark(p, 0, st);
@@ -344,10 +352,16 @@ int solve_impl(ppf_plan* p, const double* f, double* P, const double* dmx1, cons
     } else {
         rc = run_pass<float>(p, f, P, false, false, nullptr, st);
         if (rc == PPF_OK && p->d.precision == PPF_MIXED) {
+            const double ncell = (double)p->g.nx * p->g.ny * p->g.nz;
+            e = launch_sweep_gate(p->partials, p->xinv_nblk, ncell, p->scal + 5, p->flags, p->flags + 1,
+                                  p->scal + 3, p->d.sweep_tol, 1, st);
+            if (e != cudaSuccess) return cuda_fail(e, "sweep gate");
+            mark(p, 6, st);
             for (int s = 0; s < p->d.max_sweeps && rc == PPF_OK; ++s) {
                 rc = run_pass<float>(p, f, P, true, true, p->flags, st);
                 if (rc != PPF_OK) break;
-                e = launch_sweep_gate(p->scal + 1, p->flags, p->flags + 1, p->scal + 3, p->d.sweep_tol, st);
+                e = launch_sweep_gate(p->partials, p->xinv_nblk, ncell, p->scal + 5, p->flags, p->flags + 1,
+                                      p->scal + 3, p->d.sweep_tol, 0, st);
                 if (e != cudaSuccess) return cuda_fail(e, "sweep gate");
                 mark(p, 6, st);
             }

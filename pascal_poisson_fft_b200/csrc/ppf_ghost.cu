@@ -70,26 +70,48 @@ cudaError_t launch_ghosts(double* P, const Geom& g, const double* dmx1, const do
     return cudaSuccess;
 }
 
-// After a refinement sweep: record ||du||/||u_new|| and close the gate for
-// the remaining sweeps once it is below tol.  A sweep that was skipped
-// (gate already closed) leaves the record unchanged.
-__global__ void k_sweep_gate(double* norms, int* skip, int* sweeps_done, double* last_rel, double tol)
+// After an x-inverse pass that wrote per-block partial sums: reduce them in
+// a fixed order (deterministic), keep mean(u) for the next accumulate pass,
+// and after a refinement sweep count it, record ||du||/||u|| and close the
+// gate for the remaining sweeps once it is below tol.  A sweep that was
+// skipped (gate already closed) leaves everything unchanged.
+__global__ void __launch_bounds__(512) k_sweep_gate(const double* __restrict__ partials, long nblocks, double ncell,
+                                                    double* mean_prev, int* skip, int* sweeps_done, double* last_rel,
+                                                    double tol, int initial)
 {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    __shared__ double red[3][512];
     if (*skip) return;
+    double a = 0.0, b = 0.0, c = 0.0;
+    for (long i = threadIdx.x; i < nblocks; i += blockDim.x) {
+        a += partials[3 * i + 0];
+        b += partials[3 * i + 1];
+        c += partials[3 * i + 2];
+    }
+    red[0][threadIdx.x] = a; red[1][threadIdx.x] = b; red[2][threadIdx.x] = c;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) {
+            red[0][threadIdx.x] += red[0][threadIdx.x + o];
+            red[1][threadIdx.x] += red[1][threadIdx.x + o];
+            red[2][threadIdx.x] += red[2][threadIdx.x + o];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x != 0) return;
+    *mean_prev = red[2][0] / ncell;
+    if (initial) return;
     *sweeps_done += 1;
-    const double du = norms[0], u = norms[1];
+    const double du = red[0][0], u = red[1][0];
     const double rel = (u > 0.0) ? sqrt(du / u) : (du > 0.0 ? INFINITY : 0.0);
     *last_rel = rel;
     if (tol > 0.0 && rel < tol) *skip = 1;
-    norms[0] = 0.0;
-    norms[1] = 0.0;
 }
 
-cudaError_t launch_sweep_gate(double* norms, int* skip_flag, int* sweeps_done, double* last_rel, double tol,
-                              cudaStream_t st)
+cudaError_t launch_sweep_gate(const double* partials, long nblocks, double ncell, double* mean_prev, int* skip_flag,
+                              int* sweeps_done, double* last_rel, double tol, int initial, cudaStream_t st)
 {
-    k_sweep_gate<<<1, 32, 0, st>>>(norms, skip_flag, sweeps_done, last_rel, tol);
+    k_sweep_gate<<<1, 512, 0, st>>>(partials, nblocks, ncell, mean_prev, skip_flag, sweeps_done, last_rel, tol,
+                                    initial);
     return cudaGetLastError();
 }
 

@@ -43,13 +43,20 @@ cudaError_t launch_yfwd(int kind, const cx<T>* in, long in_pitch, cx<T>* out, lo
 template <typename T>
 cudaError_t launch_yinv(int kind, const cx<T>* in, long in_pitch, cx<T>* out, long out_pitch,
                         int ncols, const Geom& g, const FftSched& sch,
-                        const cx<T>* tw_ny, const cx<T>* tw_dct, const int* skip_flag, cudaStream_t st);
+                        const cx<T>* tw_ny, const cx<T>* tw_dct, const double* dc_shift,
+                        const int* skip_flag, cudaStream_t st);
 
+// x inverse into the ghosted output.  accumulate: P <- (P - *mean_prev) + du.
+// partials (optional): per-block [sum du^2, sum u^2, sum u], 3 doubles per block.
 template <typename T>
 cudaError_t launch_xinv(bool dct, const void* in, long in_pitch, double* P, const Geom& g,
-                        bool accumulate, double* norms, const FftSched& sch,
+                        bool accumulate, double* partials, const double* mean_prev, const FftSched& sch,
                         const cx<T>* tw_half, const cx<T>* tw_n, const cx<T>* tw_dct,
                         const int* skip_flag, cudaStream_t st);
+
+// blocks launch_xinv uses for geometry g (size of the partials array / 3)
+template <typename T>
+long xinv_blocks(const Geom& g);
 
 // ---- Poisson TDMA along z (ppf_tdma.cu) ----
 struct ZSys {
@@ -64,6 +71,8 @@ struct ZSys {
     double scale;         // normalisation folded into the solution
     double lowk;          // FP32 storage: systems with lam*dzmax^2 < lowk solve in FP64
     const double* dzmax2; // device scalar: max_k dx3_k^2 (written by the z-coefficient kernel)
+    double* dc_shift;     // device scalar: z-average of the (0,0) solution (subtracted by the y inverse)
+    int cyclic;           // periodic z: the reference's cyclic Thomas sequence
 };
 
 template <typename T, bool CPLX>
@@ -80,8 +89,12 @@ cudaError_t launch_ghosts(double* P, const Geom& g, const double* dmx1, const do
 cudaError_t launch_tdma_many(const double* a, const double* b, const double* c, double* d,
                              int n_sys, int n_row, bool cyclic, int* err, cudaStream_t st);
 
-// refinement bookkeeping: decides whether the next sweep runs
-cudaError_t launch_sweep_gate(double* norms, int* skip_flag, int* sweeps_done, double* last_rel,
-                              double tol, cudaStream_t st);
+// Refinement bookkeeping after an x-inverse pass with partials: reduces the
+// partials in a fixed order, stores mean(u) for the next accumulate pass,
+// and unless `initial`: counts the sweep, records ||du||/||u|| and closes
+// the gate (skip_flag) below tol.
+cudaError_t launch_sweep_gate(const double* partials, long nblocks, double ncell, double* mean_prev,
+                              int* skip_flag, int* sweeps_done, double* last_rel, double tol, int initial,
+                              cudaStream_t st);
 
 }  // namespace ppf

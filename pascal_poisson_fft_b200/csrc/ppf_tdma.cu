@@ -1,30 +1,36 @@
-// ppf_tdma.cu -- batched tridiagonal solves (sm_100a).
+// ppf_tdma.cu -- batched tridiagonal solves by the Thomas algorithm (sm_100a).
 //
-// One CTA owns S consecutive systems (consecutive wavenumbers / system
-// indices, so a warp's loads of one row are contiguous) and splits every
-// system's rows into P partitions of M rows, one partition per thread,
-// held in registers.  This is PaScaL_TDMA's distributed algorithm
-// (01_Fortran/PaScaL_TDMA/src/pascal_tdma_cuda.f90:230-269, 332-520:
-// partition-local elimination -> reduced system of 2 rows per partition ->
-// solution update) with the MPI ranks replaced by threads:
-//   1. each thread eliminates its interior rows 1..M-2 and expresses them
-//      through its own first and last unknowns
-//      (x_i = h_i - al_i x_0 - ga_i x_{M-1});
-//   2. the 2P-row reduced system of each system is solved by parallel
-//      cyclic reduction in shared memory;
-//   3. each thread updates its rows and stores them.
-// The right-hand side is read once and the solution written once.
+// One thread per system; consecutive threads own consecutive systems, so
+// every row access of a warp is one contiguous segment.  The arithmetic of
+// each row is the reference's, operation for operation
+// (01_Fortran/PaScaL_TDMA/src/tdmas.f90:114-147 tdma_many, :160-213
+// tdma_cycl_many; tdmas_cuda.f90:35-217): the first row divides by b, every
+// later row forms r = 1/(b - a c'), d' = r (d - a d'), c' = r c, and the
+// back substitution is d = d' - c' d_next.  Products and sums use explicitly
+// rounded intrinsics so the compiler cannot contract them into FMAs: the
+// solve reproduces the reference's rounding, which matters because the low
+// wavenumber systems are ill-conditioned (a different elimination order
+// changes their solution at the cond * eps level).
 //
-// k_tdma_z is the Poisson z-solve.  The coefficients of the reference's
+// The reference writes c' and d' of every row back to global memory and
+// reads them again in the back substitution.  Here the forward sweep keeps
+// only a checkpoint (c', d') every CH rows in shared memory; the backward
+// sweep re-reads the CH right-hand sides of a chunk, recomputes its c', d'
+// from the checkpoint (the same operations, so the same bits) and
+// substitutes.  Per row the field is read twice and written once.
+//
+// k_thomas_z is the Poisson z-solve: the coefficients of
 // cuda_Poisson_TDMA_z_{real,complex} (01_Fortran/src/fft_3d_poisson.f90:
-// 1121-1344) -- am = 1/(dx3_k dmx3_k), ap = 1/(dx3_k dmx3_{k+1}),
-// b = -am - ap - dxk2 - dyk2, the pin at (kx,ky,k) = (0,0,1) -- are
-// generated in registers instead of being materialised as six N-sized
-// arrays, and real and imaginary parts share one sweep.  The zero-mode mean
-// removal (cuda_Poisson_average_elimination, :628-664) and the normalisation
-// of the unnormalised inverse transforms are applied here, in spectral
-// space.  k_tdma_arr solves systems given as coefficient arrays (the
-// PaScaL_TDMA_many_solve[_cycle] replacement).
+// 1121-1344) -- am = 1/dx3_k/dmx3_k, ap = 1/dx3_k/dmx3_{k+1},
+// b = (-am - ap) - dxk2 - dyk2, the pin (a,b,c,d) = (0,1,0,0) at
+// (kx,ky,k) = (0,0,1) -- are generated in registers rather than stored as
+// six N-sized arrays, and real and imaginary parts share one sweep (they
+// are separate sweeps with identical coefficients in the reference).  The
+// thread of the (0,0) system also reports the z-average of its solution,
+// which the y-inverse pass subtracts (the arithmetic-mean removal of
+// cuda_Poisson_average_elimination, :628-664, done in spectral space).
+// k_thomas_arr / k_thomas_cycl solve systems given as coefficient arrays
+// (PaScaL_TDMA_many_solve[_cycle] replacements).
 #include "ppf_kernels.cuh"
 
 #include <math.h>
@@ -33,7 +39,23 @@ namespace ppf {
 
 namespace {
 
-constexpr int TDMA_M = 16;  // rows per partition (per thread)
+constexpr int CH = 16;  // rows per checkpoint chunk
+constexpr int TPB = 128;
+
+// explicitly rounded arithmetic (no FMA contraction) in type CT
+template <typename CT> struct R;
+template <> struct R<double> {
+    static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+    static __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+    static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+    static __device__ __forceinline__ double div(double a, double b) { return __ddiv_rn(a, b); }
+};
+template <> struct R<float> {
+    static __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+    static __device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
+    static __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+    static __device__ __forceinline__ float div(float a, float b) { return __fdiv_rn(a, b); }
+};
 
 template <typename T, bool CPLX> struct Elem;
 template <typename T> struct Elem<T, true> { using type = cx<T>; };
@@ -59,267 +81,285 @@ template <typename T> __device__ __forceinline__ void st_elem(T* p, double r, do
     *p = (T)r;
 }
 
-// Poisson coefficients: generated from the z tables and the wavenumbers.
+// Poisson coefficients of row zr (a, b, c) in CT.
 struct Coef {
     const double* am;
     const double* ap;
-    int nz;
     double lx, ly;
     bool pin;
-    __device__ __forceinline__ void get(int zr, double& a, double& b, double& cc) const
+    template <typename CT>
+    __device__ __forceinline__ void get(int zr, CT& a, CT& b, CT& c) const
     {
-        if (zr >= nz || (pin && zr == 0)) {
-            a = 0.0; b = 1.0; cc = 0.0;
+        if (pin && zr == 0) {
+            a = (CT)0; b = (CT)1; c = (CT)0;
             return;
         }
-        const double am_ = __ldg(am + zr), ap_ = __ldg(ap + zr);
-        a = am_;
-        cc = ap_;
-        b = ((-am_ - ap_) - lx) - ly;
+        const double amv = __ldg(am + zr), apv = __ldg(ap + zr);
+        a = (CT)amv;
+        c = (CT)apv;
+        // b = ac - dxk2 - dyk2 with ac = -am - ap, left to right, in CT
+        b = R<CT>::sub(R<CT>::sub(R<CT>::sub((CT)(-amv), (CT)apv), (CT)lx), (CT)ly);
     }
 };
 
-// Coefficient arrays, element (sys, row) at [row * nsys + sys]; rows
-// [row0, row0 + nrow) of the stored system are solved.  The sub-diagonal
-// of the first and the super-diagonal of the last solved row are taken as
-// zero (tdma_many never reads them; the cyclic solver moves them into its
-// second right-hand side).
-struct CoefArr {
-    const double* a;
-    const double* b;
-    const double* c;
-    long nsys, sys;
-    int row0, nrow;
-    __device__ __forceinline__ void get(int zr, double& av, double& bv, double& cv) const
-    {
-        if (zr >= nrow) {
-            av = 0.0; bv = 1.0; cv = 0.0;
-            return;
+// One Thomas forward step on row state (c', d'): first row (zr == 0) divides.
+template <typename CT, bool CPLX>
+__device__ __forceinline__ void fwd_row(bool first, CT a, CT b, CT c, CT dr_in, CT di_in, CT& cp, CT& dr, CT& di)
+{
+    if (first) {
+        dr = R<CT>::div(dr_in, b);
+        if (CPLX) di = R<CT>::div(di_in, b);
+        cp = R<CT>::div(c, b);
+    } else {
+        const CT r = R<CT>::div((CT)1, R<CT>::sub(b, R<CT>::mul(a, cp)));
+        dr = R<CT>::mul(r, R<CT>::sub(dr_in, R<CT>::mul(a, dr)));
+        if (CPLX) di = R<CT>::mul(r, R<CT>::sub(di_in, R<CT>::mul(a, di)));
+        cp = R<CT>::mul(r, c);
+    }
+}
+
+// The whole z-solve of one Poisson system in arithmetic type CT.
+// ck: this thread's checkpoint column (stride TPB), 3 values per chunk.
+template <typename T, typename CT, bool CPLX>
+__device__ __forceinline__ void thomas_poisson(typename Elem<T, CPLX>::type* data, long sys, long plane, int nz,
+                                               const Coef& co, double scale, double* ck, double& zsum, bool& bad)
+{
+    const int nch = (nz + CH - 1) / CH;
+    CT cp = 0, dr = 0, di = 0;
+    // forward sweep
+    for (int ch = 0; ch < nch; ++ch) {
+        const int z0 = ch * CH;
+        double vr[CH], vi[CH];
+#pragma unroll
+        for (int r = 0; r < CH; ++r) {
+            vr[r] = 0.0; vi[r] = 0.0;
+            if (z0 + r < nz) ld_elem<T>(data + (long)(z0 + r) * plane + sys, vr[r], vi[r]);
         }
-        const long o = (long)(zr + row0) * nsys + sys;
-        av = (zr == 0) ? 0.0 : __ldg(a + o);
-        bv = __ldg(b + o);
-        cv = (zr == nrow - 1) ? 0.0 : __ldg(c + o);
-    }
-};
-
-// Partition-local elimination in arithmetic type CT.  On return dr/di hold
-// h, al holds alpha, ga holds gamma for rows 1..M-2, and the two reduced
-// rows (F: first, L: last; sub, diag, super, rhs_re, rhs_im) are returned.
-template <typename CT, int M, bool CPLX, typename CO>
-__device__ __forceinline__ void eliminate(const CO& co, int z0, double* dr, double* di, double* al, double* ga,
-                                          double* F, double* L)
-{
-    double a0, b0, c0, a1, b1, c1;
-    co.get(z0, a0, b0, c0);
-    co.get(z0 + 1, a1, b1, c1);
-    {
-        const CT ib = (CT)1 / (CT)b1;
-        ga[1] = (double)((CT)c1 * ib);
-        al[1] = (double)((CT)a1 * ib);
-        dr[1] = (double)((CT)dr[1] * ib);
-        if (CPLX) di[1] = (double)((CT)di[1] * ib);
-    }
 #pragma unroll
-    for (int r = 2; r <= M - 2; ++r) {
-        double a, b, c;
-        co.get(z0 + r, a, b, c);
-        const CT rr = (CT)1 / ((CT)b - (CT)a * (CT)ga[r - 1]);
-        dr[r] = (double)(rr * ((CT)dr[r] - (CT)a * (CT)dr[r - 1]));
-        if (CPLX) di[r] = (double)(rr * ((CT)di[r] - (CT)a * (CT)di[r - 1]));
-        ga[r] = (double)(rr * (CT)c);
-        al[r] = (double)(-rr * (CT)a * (CT)al[r - 1]);
-    }
-    double aL, bL, cL;
-    co.get(z0 + M - 1, aL, bL, cL);
-#pragma unroll
-    for (int r = M - 3; r >= 1; --r) {
-        const CT e = (CT)ga[r];
-        dr[r] = (double)((CT)dr[r] - e * (CT)dr[r + 1]);
-        if (CPLX) di[r] = (double)((CT)di[r] - e * (CT)di[r + 1]);
-        al[r] = (double)((CT)al[r] - e * (CT)al[r + 1]);
-        ga[r] = (double)(-e * (CT)ga[r + 1]);
-    }
-    // F couples (L_{p-1}, x_0, x_{M-1}); L couples (x_0, x_{M-1}, F_{p+1})
-    F[0] = a0;
-    F[1] = (double)((CT)b0 - (CT)c0 * (CT)al[1]);
-    F[2] = (double)(-(CT)c0 * (CT)ga[1]);
-    F[3] = (double)((CT)dr[0] - (CT)c0 * (CT)dr[1]);
-    F[4] = CPLX ? (double)((CT)di[0] - (CT)c0 * (CT)di[1]) : 0.0;
-    L[0] = (double)(-(CT)aL * (CT)al[M - 2]);
-    L[1] = (double)((CT)bL - (CT)aL * (CT)ga[M - 2]);
-    L[2] = cL;
-    L[3] = (double)((CT)dr[M - 1] - (CT)aL * (CT)dr[M - 2]);
-    L[4] = CPLX ? (double)((CT)di[M - 1] - (CT)aL * (CT)di[M - 2]) : 0.0;
-}
-
-// Parallel cyclic reduction of the 2P-row reduced systems of S systems in
-// shared memory (two buffers of 4 * 2P * S doubles; rows stored with a unit
-// diagonal).  Thread (sl, p) supplies rows 2p (F) and 2p+1 (L) and receives
-// their solutions.  Returns the buffer that does not hold the result.
-__device__ __forceinline__ double* reduced_solve(double* sh, int p, int sl, int S, int P, const double* F,
-                                                 const double* L, double& x0r, double& x0i, double& xLr,
-                                                 double& xLi)
-{
-    const int n2 = 2 * P;
-    const int NS = n2 * S;
-    double* src = sh;
-    double* dst = sh + 4 * NS;
-    {
-        const double iF = 1.0 / F[1], iL = 1.0 / L[1];
-        const int qF = (2 * p) * S + sl, qL = (2 * p + 1) * S + sl;
-        src[qF] = F[0] * iF; src[NS + qF] = F[2] * iF; src[2 * NS + qF] = F[3] * iF; src[3 * NS + qF] = F[4] * iF;
-        src[qL] = L[0] * iL; src[NS + qL] = L[2] * iL; src[2 * NS + qL] = L[3] * iL; src[3 * NS + qL] = L[4] * iL;
-    }
-    __syncthreads();
-    for (int d = 1; d < n2; d <<= 1) {
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int i = 2 * p + h;
-            const int q = i * S + sl;
-            const double ai = src[q], ci = src[NS + q], dri = src[2 * NS + q], dii = src[3 * NS + q];
-            double am_ = 0, cm_ = 0, drm = 0, dim_ = 0, ap_ = 0, cp_ = 0, drp = 0, dip = 0;
-            if (i - d >= 0) {
-                const int qm = (i - d) * S + sl;
-                am_ = src[qm]; cm_ = src[NS + qm]; drm = src[2 * NS + qm]; dim_ = src[3 * NS + qm];
+        for (int r = 0; r < CH; ++r) {
+            const int zr = z0 + r;
+            if (zr < nz) {
+                CT a, b, c;
+                co.get<CT>(zr, a, b, c);
+                const bool pinrow = co.pin && zr == 0;
+                fwd_row<CT, CPLX>(zr == 0, a, b, c, pinrow ? (CT)0 : (CT)vr[r], pinrow ? (CT)0 : (CT)vi[r], cp, dr, di);
             }
-            if (i + d < n2) {
-                const int qp = (i + d) * S + sl;
-                ap_ = src[qp]; cp_ = src[NS + qp]; drp = src[2 * NS + qp]; dip = src[3 * NS + qp];
-            }
-            const double ib = 1.0 / (1.0 - ai * cm_ - ci * ap_);
-            dst[q] = -ai * am_ * ib;
-            dst[NS + q] = -ci * cp_ * ib;
-            dst[2 * NS + q] = (dri - ai * drm - ci * drp) * ib;
-            dst[3 * NS + q] = (dii - ai * dim_ - ci * dip) * ib;
         }
-        __syncthreads();
-        double* t = src; src = dst; dst = t;
+        ck[(3 * ch + 0) * TPB] = (double)cp;
+        ck[(3 * ch + 1) * TPB] = (double)dr;
+        ck[(3 * ch + 2) * TPB] = (double)di;
     }
-    x0r = src[2 * NS + (2 * p) * S + sl];
-    x0i = src[3 * NS + (2 * p) * S + sl];
-    xLr = src[2 * NS + (2 * p + 1) * S + sl];
-    xLi = src[3 * NS + (2 * p + 1) * S + sl];
-    return dst;
-}
-
-template <int M, bool CPLX>
-__device__ __forceinline__ void update_rows(double* dr, double* di, const double* al, const double* ga, double x0r,
-                                            double x0i, double xLr, double xLi)
-{
-    dr[0] = x0r; di[0] = x0i;
+    // backward sweep, chunk by chunk from the top
+    CT xr = 0, xi = 0;
+    for (int ch = nch - 1; ch >= 0; --ch) {
+        const int z0 = ch * CH;
+        CT c_[CH], r_[CH], i_[CH];
+        double vr[CH], vi[CH];
 #pragma unroll
-    for (int r = 1; r <= M - 2; ++r) {
-        dr[r] = dr[r] - al[r] * x0r - ga[r] * xLr;
-        if (CPLX) di[r] = di[r] - al[r] * x0i - ga[r] * xLi;
+        for (int r = 0; r < CH; ++r) {
+            vr[r] = 0.0; vi[r] = 0.0;
+            if (z0 + r < nz) ld_elem<T>(data + (long)(z0 + r) * plane + sys, vr[r], vi[r]);
+        }
+        CT pcp = 0, pdr = 0, pdi = 0;
+        if (ch > 0) {
+            pcp = (CT)ck[(3 * (ch - 1) + 0) * TPB];
+            pdr = (CT)ck[(3 * (ch - 1) + 1) * TPB];
+            pdi = (CT)ck[(3 * (ch - 1) + 2) * TPB];
+        }
+#pragma unroll
+        for (int r = 0; r < CH; ++r) {
+            const int zr = z0 + r;
+            if (zr < nz) {
+                CT a, b, c;
+                co.get<CT>(zr, a, b, c);
+                const bool pinrow = co.pin && zr == 0;
+                fwd_row<CT, CPLX>(zr == 0, a, b, c, pinrow ? (CT)0 : (CT)vr[r], pinrow ? (CT)0 : (CT)vi[r], pcp, pdr,
+                                  pdi);
+            }
+            c_[r] = pcp; r_[r] = pdr; i_[r] = pdi;
+        }
+#pragma unroll
+        for (int r = CH - 1; r >= 0; --r) {
+            const int zr = z0 + r;
+            if (zr < nz) {
+                if (zr == nz - 1) {
+                    xr = r_[r];
+                    xi = i_[r];
+                } else {
+                    xr = R<CT>::sub(r_[r], R<CT>::mul(c_[r], xr));
+                    if (CPLX) xi = R<CT>::sub(i_[r], R<CT>::mul(c_[r], xi));
+                }
+                const double sr = (double)xr * scale, si = (double)xi * scale;
+                zsum += sr;
+                if (!isfinite(sr) || !isfinite(si)) bad = true;
+                st_elem<T>(data + (long)zr * plane + sys, sr, si);
+            }
+        }
     }
-    dr[M - 1] = xLr; di[M - 1] = xLi;
 }
 
-// Partitions / systems per CTA for n rows: P = ceil(n/M) partitions, S a
-// power of two with S*P <= 256.
-inline bool tdma_shape(int nrows, int& P, int& S, int& lgS)
+// Periodic z: the reference routes the solve through the cyclic Thomas
+// algorithm (cuda_ptdma_core, fft_3d_poisson.f90:898-913 ->
+// tdma_cycl_many_cuda) even though its coefficients zero am at k=1 and ap at
+// k=n3m.  Reproduced here operation for operation (tdmas.f90:160-213):
+// rows 1..nz-1 are swept for d and e (e_1 = -a_1, e_{nz-1} = -c_{nz-1}),
+// x_0 is formed from the back-substituted d_1, e_1, then x_i = d_i + x_0 e_i.
+// The back substitution runs twice (first for d_1, e_1) instead of storing e.
+template <typename T, typename CT, bool CPLX>
+__device__ __forceinline__ void thomas_poisson_cyc(typename Elem<T, CPLX>::type* data, long sys, long plane, int nz,
+                                                   const Coef& co, double scale, double* ck, double& zsum, bool& bad)
 {
-    P = (nrows + TDMA_M - 1) / TDMA_M;
-    if (P > 64 || P < 1) return false;
-    S = 1;
-    while (S * 2 * P <= 256 && S < 128) S *= 2;
-    lgS = 0;
-    while ((1 << lgS) < S) ++lgS;
-    return true;
+    const int m = nz - 1;
+    const int nch = (m + CH - 1) / CH;
+    CT a1, b1, c1, an, bn, cn;
+    co.get<CT>(1, a1, b1, c1);
+    co.get<CT>(nz - 1, an, bn, cn);
+    const CT e_first = -a1, e_last = -cn;
+    auto e_in = [&](int q) -> CT { return (q == m - 1) ? e_last : ((q == 0) ? e_first : (CT)0); };
+    CT cp = 0, dr = 0, di = 0, ep = 0, dum = 0;
+    for (int ch = 0; ch < nch; ++ch) {
+        const int q0 = ch * CH;
+        double vr[CH], vi[CH];
+#pragma unroll
+        for (int r = 0; r < CH; ++r) {
+            vr[r] = 0.0; vi[r] = 0.0;
+            if (q0 + r < m) ld_elem<T>(data + (long)(q0 + r + 1) * plane + sys, vr[r], vi[r]);
+        }
+#pragma unroll
+        for (int r = 0; r < CH; ++r) {
+            const int q = q0 + r;
+            if (q < m) {
+                CT a, b, c;
+                co.get<CT>(q + 1, a, b, c);
+                CT cpe = cp;
+                fwd_row<CT, CPLX>(q == 0, a, b, c, (CT)vr[r], (CT)vi[r], cp, dr, di);
+                fwd_row<CT, false>(q == 0, a, b, c, e_in(q), (CT)0, cpe, ep, dum);
+            }
+        }
+        ck[(4 * ch + 0) * TPB] = (double)cp;
+        ck[(4 * ch + 1) * TPB] = (double)dr;
+        ck[(4 * ch + 2) * TPB] = (double)di;
+        ck[(4 * ch + 3) * TPB] = (double)ep;
+    }
+    const CT dtop_r = dr, dtop_i = di, etop = ep;
+    CT d1r = 0, d1i = 0, e1 = 0;
+    double x0r = 0.0, x0i = 0.0;
+    for (int pass = 0; pass < 2; ++pass) {
+        if (pass == 1) {
+            CT a0, b0, c0;
+            co.get<CT>(0, a0, b0, c0);
+            double v0r = 0.0, v0i = 0.0;
+            if (!(co.pin)) ld_elem<T>(data + sys, v0r, v0i);
+            const CT den = R<CT>::add(R<CT>::add(b0, R<CT>::mul(a0, etop)), R<CT>::mul(c0, e1));
+            x0r = (double)R<CT>::div(R<CT>::sub(R<CT>::sub((CT)v0r, R<CT>::mul(a0, dtop_r)), R<CT>::mul(c0, d1r)), den);
+            x0i = (double)R<CT>::div(R<CT>::sub(R<CT>::sub((CT)v0i, R<CT>::mul(a0, dtop_i)), R<CT>::mul(c0, d1i)), den);
+        }
+        CT yr = 0, yi = 0, ye = 0;
+        for (int ch = nch - 1; ch >= 0; --ch) {
+            const int q0 = ch * CH;
+            double vr[CH], vi[CH];
+#pragma unroll
+            for (int r = 0; r < CH; ++r) {
+                vr[r] = 0.0; vi[r] = 0.0;
+                if (q0 + r < m) ld_elem<T>(data + (long)(q0 + r + 1) * plane + sys, vr[r], vi[r]);
+            }
+            CT pc = 0, pr = 0, pi = 0, pe = 0;
+            if (ch > 0) {
+                pc = (CT)ck[(4 * (ch - 1) + 0) * TPB];
+                pr = (CT)ck[(4 * (ch - 1) + 1) * TPB];
+                pi = (CT)ck[(4 * (ch - 1) + 2) * TPB];
+                pe = (CT)ck[(4 * (ch - 1) + 3) * TPB];
+            }
+            CT c_[CH], r_[CH], i_[CH], e_[CH];
+#pragma unroll
+            for (int r = 0; r < CH; ++r) {
+                const int q = q0 + r;
+                if (q < m) {
+                    CT a, b, c;
+                    co.get<CT>(q + 1, a, b, c);
+                    CT pce = pc;
+                    fwd_row<CT, CPLX>(q == 0, a, b, c, (CT)vr[r], (CT)vi[r], pc, pr, pi);
+                    fwd_row<CT, false>(q == 0, a, b, c, e_in(q), (CT)0, pce, pe, dum);
+                }
+                c_[r] = pc; r_[r] = pr; i_[r] = pi; e_[r] = pe;
+            }
+#pragma unroll
+            for (int r = CH - 1; r >= 0; --r) {
+                const int q = q0 + r;
+                if (q < m) {
+                    if (q == m - 1) { yr = r_[r]; yi = i_[r]; ye = e_[r]; }
+                    else {
+                        yr = R<CT>::sub(r_[r], R<CT>::mul(c_[r], yr));
+                        if (CPLX) yi = R<CT>::sub(i_[r], R<CT>::mul(c_[r], yi));
+                        ye = R<CT>::sub(e_[r], R<CT>::mul(c_[r], ye));
+                    }
+                    if (pass == 1) {
+                        const CT xr = R<CT>::add(yr, R<CT>::mul((CT)x0r, ye));
+                        const CT xi = CPLX ? R<CT>::add(yi, R<CT>::mul((CT)x0i, ye)) : (CT)0;
+                        const double sr = (double)xr * scale, si = (double)xi * scale;
+                        zsum += sr;
+                        if (!isfinite(sr) || !isfinite(si)) bad = true;
+                        st_elem<T>(data + (long)(q + 1) * plane + sys, sr, si);
+                    }
+                }
+            }
+        }
+        if (pass == 0) { d1r = yr; d1i = yi; e1 = ye; }
+    }
+    const double sr = x0r * scale, si = x0i * scale;
+    zsum += sr;
+    if (!isfinite(sr) || !isfinite(si)) bad = true;
+    st_elem<T>(data + sys, sr, si);
 }
 
 }  // namespace
 
 template <typename T, bool CPLX>
-__global__ void __launch_bounds__(256) k_tdma_z(void* __restrict__ data_, ZSys z, int lgS,
-                                                const int* __restrict__ skip, int* __restrict__ err)
+__global__ void __launch_bounds__(TPB) k_thomas_z(void* __restrict__ data_, ZSys z, const int* __restrict__ skip,
+                                                  int* __restrict__ err)
 {
-    constexpr int M = TDMA_M;
     if (skip && *skip) return;
-    extern __shared__ double sh[];
+    extern __shared__ double ck[];
     using E = typename Elem<T, CPLX>::type;
     E* data = reinterpret_cast<E*>(data_);
-
-    const int S = 1 << lgS;
-    const int P = blockDim.x >> lgS;
-    const int sl = threadIdx.x & (S - 1), p = threadIdx.x >> lgS;
-    const long sys = (long)blockIdx.x * S + sl;
+    const long sys = (long)blockIdx.x * TPB + threadIdx.x;
     const int kx = (int)(sys % z.pitch), ky = (int)(sys / z.pitch);
     const bool valid = (kx < z.mx) && (ky < z.my);
+    if (!valid) return;
 
     Coef co;
-    co.am = z.am; co.ap = z.ap; co.nz = z.nz;
-    co.lx = valid ? z.lamx[kx] : 0.0;
-    co.ly = valid ? z.lamy[ky] : 0.0;
-    co.pin = valid && kx == 0 && ky == 0;
-
-    const int z0 = p * M;
-    double dr[M], di[M], al[M], ga[M];
-#pragma unroll
-    for (int r = 0; r < M; ++r) {
-        const int zr = z0 + r;
-        dr[r] = 0.0; di[r] = 0.0;
-        if (valid && zr < z.nz && !(co.pin && zr == 0)) ld_elem<T>(data + (long)zr * z.plane + sys, dr[r], di[r]);
-    }
-
-    double F[5], L[5];
+    co.am = z.am; co.ap = z.ap;
+    co.lx = z.lamx[kx];
+    co.ly = z.lamy[ky];
+    co.pin = (kx == 0 && ky == 0);
     const bool fp64 = (sizeof(T) == 8) || ((co.lx + co.ly) * __ldg(z.dzmax2) < z.lowk);
-    if (fp64) eliminate<double, M, CPLX, Coef>(co, z0, dr, di, al, ga, F, L);
-    else      eliminate<float, M, CPLX, Coef>(co, z0, dr, di, al, ga, F, L);
-
-    double x0r, x0i, xLr, xLi;
-    double* freebuf = reduced_solve(sh, p, sl, S, P, F, L, x0r, x0i, xLr, xLi);
-    update_rows<M, CPLX>(dr, di, al, ga, x0r, x0i, xLr, xLi);
-
-    // zero mode: subtract the z-average of (kx,ky)=(0,0), i.e. the
-    // arithmetic mean of u over all cells
-    if (blockIdx.x == 0) {
-        double part = 0.0;
-        if (sl == 0) {
-#pragma unroll
-            for (int r = 0; r < M; ++r)
-                if (z0 + r < z.nz) part += dr[r];
-            freebuf[p] = part;
-        }
-        __syncthreads();
-        if (sl == 0) {
-            double tot = 0.0;
-            for (int q = 0; q < P; ++q) tot += freebuf[q];
-            const double mean = tot / (double)z.nz;
-#pragma unroll
-            for (int r = 0; r < M; ++r) dr[r] -= mean;
-        }
-    }
-
+    double zsum = 0.0;
     bool bad = false;
-#pragma unroll
-    for (int r = 0; r < M; ++r) {
-        const int zr = z0 + r;
-        if (valid && zr < z.nz) {
-            const double vr = dr[r] * z.scale, vi = di[r] * z.scale;
-            if (!isfinite(vr) || !isfinite(vi)) bad = true;
-            st_elem<T>(data + (long)zr * z.plane + sys, vr, vi);
-        }
+    if (z.cyclic) {
+        if (fp64) thomas_poisson_cyc<T, double, CPLX>(data, sys, z.plane, z.nz, co, z.scale, ck + threadIdx.x, zsum, bad);
+        else      thomas_poisson_cyc<T, float, CPLX>(data, sys, z.plane, z.nz, co, z.scale, ck + threadIdx.x, zsum, bad);
+    } else {
+        if (fp64) thomas_poisson<T, double, CPLX>(data, sys, z.plane, z.nz, co, z.scale, ck + threadIdx.x, zsum, bad);
+        else      thomas_poisson<T, float, CPLX>(data, sys, z.plane, z.nz, co, z.scale, ck + threadIdx.x, zsum, bad);
     }
+    if (co.pin && z.dc_shift) *z.dc_shift = zsum / (double)z.nz;
     if (bad && err) atomicOr(err, 1);
 }
 
 template <typename T, bool CPLX>
 cudaError_t launch_tdma_z(void* data, const ZSys& z, const int* skip_flag, int* err_flag, cudaStream_t st)
 {
-    int P, S, lgS;
-    if (!tdma_shape(z.nz, P, S, lgS)) return cudaErrorInvalidConfiguration;  // nz <= 1024
-    const int threads = S * P;
-    const size_t smem = (size_t)2 * 4 * (2 * P) * S * sizeof(double);
+    const int nch = (z.nz + CH - 1) / CH;
+    const size_t smem = (size_t)(z.cyclic ? 4 : 3) * nch * TPB * sizeof(double);
+    if (smem > 200 * 1024) return cudaErrorInvalidConfiguration;
     const long nsys = z.plane;  // pitch * my systems incl. padding columns
-    dim3 grid((unsigned)((nsys + S - 1) / S));
-    auto kern = k_tdma_z<T, CPLX>;
+    dim3 grid((unsigned)((nsys + TPB - 1) / TPB));
+    auto kern = k_thomas_z<T, CPLX>;
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
-    kern<<<grid, threads, smem, st>>>(data, z, lgS, skip_flag, err_flag);
+    kern<<<grid, TPB, smem, st>>>(data, z, skip_flag, err_flag);
     return cudaGetLastError();
 }
 
@@ -329,117 +369,176 @@ template cudaError_t launch_tdma_z<float, true>(void*, const ZSys&, const int*, 
 template cudaError_t launch_tdma_z<float, false>(void*, const ZSys&, const int*, int*, cudaStream_t);
 
 // --------------------------------------------------------------------------
-// Coefficient-array solves (PaScaL_TDMA_many_solve / _cycle replacement).
-//   non-cyclic: rows 0..n-1, right-hand side d.
-//   cyclic    : the method of tdma_cycl_many (01_Fortran/PaScaL_TDMA/src/
-//               tdmas.f90:160-213): rows 1..n-1 are solved for two
-//               right-hand sides, d and e (e_1 = -a_1, e_{n-1} = -c_{n-1}),
-//               then x_0 = (d_0 - a_0 d'_{n-1} - c_0 d'_1) /
-//                          (b_0 + a_0 e'_{n-1} + c_0 e'_1),
-//               x_i = d'_i + x_0 e'_i.  Both right-hand sides share one
-//               sweep (as the real/imaginary pair of the complex path) and
-//               the correction is applied before the store, so neither a
-//               scratch e-array nor a second pass is needed.
+// Coefficient-array solves, element (sys, row) at [row * n_sys + sys].
 // --------------------------------------------------------------------------
-template <bool CYC>
-__global__ void __launch_bounds__(256) k_tdma_arr(const double* __restrict__ a, const double* __restrict__ b,
-                                                  const double* __restrict__ c, double* __restrict__ d, int n_sys,
-                                                  int n_row, int lgS, int* __restrict__ err)
+namespace {
+
+struct ArrIn {
+    const double* a;
+    const double* b;
+    const double* c;
+    double* d;
+    long ns, sys;
+};
+
+// loads CH rows [z0, z0+CH) of a, b, c, d (rows >= n are zero)
+__device__ __forceinline__ void ld_chunk(const ArrIn& A, int z0, int n, double* a, double* b, double* c, double* d)
 {
-    constexpr int M = TDMA_M;
-    extern __shared__ double sh[];
-    const int S = 1 << lgS;
-    const int P = blockDim.x >> lgS;
-    const int sl = threadIdx.x & (S - 1), p = threadIdx.x >> lgS;
-    const long sysl = (long)blockIdx.x * S + sl;
-    const bool valid = sysl < n_sys;
-    const long sys = valid ? sysl : 0;
-
-    CoefArr co;
-    co.a = a; co.b = b; co.c = c; co.nsys = n_sys; co.sys = sys;
-    co.row0 = CYC ? 1 : 0;
-    co.nrow = CYC ? n_row - 1 : n_row;
-
-    const int z0 = p * M;
-    double dr[M], di[M], al[M], ga[M];
 #pragma unroll
-    for (int r = 0; r < M; ++r) {
-        const int zr = z0 + r;
-        dr[r] = 0.0; di[r] = 0.0;
-        if (zr < co.nrow) {
-            const long o = (long)(zr + co.row0) * n_sys + sys;
-            dr[r] = d[o];
-            if (CYC) {
-                if (zr == 0) di[r] -= __ldg(a + o);
-                if (zr == co.nrow - 1) di[r] -= __ldg(c + o);
-            }
+    for (int r = 0; r < CH; ++r) {
+        a[r] = 0.0; b[r] = 1.0; c[r] = 0.0; d[r] = 0.0;
+        if (z0 + r < n) {
+            const long o = (long)(z0 + r) * A.ns + A.sys;
+            a[r] = __ldg(A.a + o); b[r] = __ldg(A.b + o); c[r] = __ldg(A.c + o); d[r] = A.d[o];
         }
     }
-    double F[5], L[5];
-    eliminate<double, M, CYC, CoefArr>(co, z0, dr, di, al, ga, F, L);
-    double x0r, x0i, xLr, xLi;
-    double* freebuf = reduced_solve(sh, p, sl, S, P, F, L, x0r, x0i, xLr, xLi);
-    update_rows<M, CYC>(dr, di, al, ga, x0r, x0i, xLr, xLi);
+}
 
-    double xfirst = 0.0;
-    if (CYC) {
-        // d'_1, e'_1 live in partition 0 (local row 0); d'_{n-1}, e'_{n-1}
-        // in partition (n-2)/M at local row (n-2)%M
-        const int last = co.nrow - 1;
-        const int pl = last / M, rl = last % M;
-        if (p == 0) { freebuf[sl] = dr[0]; freebuf[S + sl] = di[0]; }
-        if (p == pl) {
+}  // namespace
+
+// tdma_many (tdmas.f90:114-147)
+__global__ void __launch_bounds__(TPB) k_thomas_arr(const double* __restrict__ a, const double* __restrict__ b,
+                                                    const double* __restrict__ c, double* __restrict__ d, int n_sys,
+                                                    int n)
+{
+    extern __shared__ double ck[];
+    const long sys = (long)blockIdx.x * TPB + threadIdx.x;
+    if (sys >= n_sys) return;
+    double* my = ck + threadIdx.x;
+    ArrIn A{ a, b, c, d, n_sys, sys };
+    const int nch = (n + CH - 1) / CH;
+    double cp = 0, dp = 0, dum = 0;
+    double av[CH], bv[CH], cv[CH], dv[CH];
+    for (int ch = 0; ch < nch; ++ch) {
+        const int z0 = ch * CH;
+        ld_chunk(A, z0, n, av, bv, cv, dv);
 #pragma unroll
-            for (int r = 0; r < M; ++r)
-                if (r == rl) { freebuf[2 * S + sl] = dr[r]; freebuf[3 * S + sl] = di[r]; }
-        }
-        __syncthreads();
-        if (valid) {
-            const double d1 = freebuf[sl], e1 = freebuf[S + sl];
-            const double dn = freebuf[2 * S + sl], en = freebuf[3 * S + sl];
-            const double a0 = __ldg(a + sys), b0 = __ldg(b + sys), c0 = __ldg(c + sys), d0 = d[sys];
-            xfirst = (d0 - a0 * dn - c0 * d1) / (b0 + a0 * en + c0 * e1);
-        }
-        __syncthreads();  // every thread has read d_0 before partition 0 stores x_0
+        for (int r = 0; r < CH; ++r)
+            if (z0 + r < n) fwd_row<double, false>(z0 + r == 0, av[r], bv[r], cv[r], dv[r], 0.0, cp, dp, dum);
+        my[(2 * ch) * TPB] = cp;
+        my[(2 * ch + 1) * TPB] = dp;
     }
-    bool bad = false;
-    if (valid) {
+    double x = 0;
+    for (int ch = nch - 1; ch >= 0; --ch) {
+        const int z0 = ch * CH;
+        ld_chunk(A, z0, n, av, bv, cv, dv);
+        double pc = 0, pd = 0;
+        if (ch > 0) { pc = my[(2 * ch - 2) * TPB]; pd = my[(2 * ch - 1) * TPB]; }
+        double c_[CH], d_[CH];
 #pragma unroll
-        for (int r = 0; r < M; ++r) {
+        for (int r = 0; r < CH; ++r) {
+            if (z0 + r < n) fwd_row<double, false>(z0 + r == 0, av[r], bv[r], cv[r], dv[r], 0.0, pc, pd, dum);
+            c_[r] = pc; d_[r] = pd;
+        }
+#pragma unroll
+        for (int r = CH - 1; r >= 0; --r) {
             const int zr = z0 + r;
-            if (zr < co.nrow) {
-                const double x = CYC ? dr[r] + xfirst * di[r] : dr[r];
-                if (!isfinite(x)) bad = true;
-                d[(long)(zr + co.row0) * n_sys + sys] = x;
+            if (zr < n) {
+                x = (zr == n - 1) ? d_[r] : __dsub_rn(d_[r], __dmul_rn(c_[r], x));
+                d[(long)zr * n_sys + sys] = x;
             }
         }
-        if (CYC && p == 0) d[sys] = xfirst;
     }
-    if (bad && err) atomicOr(err, 1);
+}
+
+// tdma_cycl_many (tdmas.f90:160-213): rows 1..n-1 are swept for the
+// right-hand sides d and e (e_1 = -a_1, e_{n-1} = -c_{n-1}); x_0 needs the
+// back-substituted d_1, e_1, so the back substitution runs twice (first to
+// obtain them, then to write x_i = d_i + x_0 e_i) instead of storing e.
+__global__ void __launch_bounds__(TPB) k_thomas_cycl(const double* __restrict__ a, const double* __restrict__ b,
+                                                     const double* __restrict__ c, double* __restrict__ d,
+                                                     int n_sys, int n)
+{
+    extern __shared__ double ck[];
+    const long sys = (long)blockIdx.x * TPB + threadIdx.x;
+    if (sys >= n_sys) return;
+    double* my = ck + threadIdx.x;
+    // view of rows 1..n-1 as a system of m = n-1 rows
+    ArrIn A{ a + n_sys, b + n_sys, c + n_sys, d + n_sys, n_sys, sys };
+    const int m = n - 1;
+    const int nch = (m + CH - 1) / CH;
+    double av[CH], bv[CH], cv[CH], dv[CH];
+    const double e_first = -__ldg(a + n_sys + sys);                // -a(2)
+    const double e_last = -__ldg(c + (long)(n - 1) * n_sys + sys);  // -c(n2)
+    auto e_in = [&](int zr) -> double {
+        // e(2) = -a(2) is set before e(n2) = -c(n2) (tdmas.f90:172-174)
+        if (zr == m - 1) return e_last;
+        if (zr == 0) return e_first;
+        return 0.0;
+    };
+    double cp = 0, dp = 0, ep = 0;
+    for (int ch = 0; ch < nch; ++ch) {
+        const int z0 = ch * CH;
+        ld_chunk(A, z0, m, av, bv, cv, dv);
+#pragma unroll
+        for (int r = 0; r < CH; ++r)
+            if (z0 + r < m) fwd_row<double, true>(z0 + r == 0, av[r], bv[r], cv[r], dv[r], e_in(z0 + r), cp, dp, ep);
+        my[(3 * ch) * TPB] = cp;
+        my[(3 * ch + 1) * TPB] = dp;
+        my[(3 * ch + 2) * TPB] = ep;
+    }
+    // pass 1: d_1, e_1 after back substitution (d_{n-1}, e_{n-1} are d', e' of the top row)
+    const double d_top = dp, e_top = ep;
+    double xd = 0, xe = 0;
+    for (int pass = 0; pass < 2; ++pass) {
+        double x0 = 0.0;
+        if (pass == 1) {
+            const double a0 = __ldg(a + sys), b0 = __ldg(b + sys), c0 = __ldg(c + sys), d0 = d[sys];
+            // d(1) = (d(1) - a(1) d(n2) - c(1) d(2)) / (b(1) + a(1) e(n2) + c(1) e(2))
+            x0 = __ddiv_rn(__dsub_rn(__dsub_rn(d0, __dmul_rn(a0, d_top)), __dmul_rn(c0, xd)),
+                           __dadd_rn(__dadd_rn(b0, __dmul_rn(a0, e_top)), __dmul_rn(c0, xe)));
+        }
+        double yd = 0, ye = 0;
+        for (int ch = nch - 1; ch >= 0; --ch) {
+            const int z0 = ch * CH;
+            ld_chunk(A, z0, m, av, bv, cv, dv);
+            double pc = 0, pd = 0, pe = 0;
+            if (ch > 0) { pc = my[(3 * ch - 3) * TPB]; pd = my[(3 * ch - 2) * TPB]; pe = my[(3 * ch - 1) * TPB]; }
+            double c_[CH], d_[CH], e_[CH];
+#pragma unroll
+            for (int r = 0; r < CH; ++r) {
+                if (z0 + r < m) fwd_row<double, true>(z0 + r == 0, av[r], bv[r], cv[r], dv[r], e_in(z0 + r), pc, pd, pe);
+                c_[r] = pc; d_[r] = pd; e_[r] = pe;
+            }
+#pragma unroll
+            for (int r = CH - 1; r >= 0; --r) {
+                const int zr = z0 + r;
+                if (zr < m) {
+                    if (zr == m - 1) { yd = d_[r]; ye = e_[r]; }
+                    else {
+                        yd = __dsub_rn(d_[r], __dmul_rn(c_[r], yd));
+                        ye = __dsub_rn(e_[r], __dmul_rn(c_[r], ye));
+                    }
+                    if (pass == 1) d[(long)(zr + 1) * n_sys + sys] = __dadd_rn(yd, __dmul_rn(x0, ye));
+                }
+            }
+        }
+        if (pass == 0) { xd = yd; xe = ye; }
+        else d[sys] = x0;
+    }
 }
 
 cudaError_t launch_tdma_many(const double* a, const double* b, const double* c, double* d, int n_sys, int n_row,
                              bool cyclic, int* err, cudaStream_t st)
 {
-    int P, S, lgS;
-    if (!tdma_shape(cyclic ? n_row - 1 : n_row, P, S, lgS)) return cudaErrorInvalidConfiguration;
-    const int threads = S * P;
-    const size_t smem = (size_t)2 * 4 * (2 * P) * S * sizeof(double);
-    dim3 grid((unsigned)(((long)n_sys + S - 1) / S));
+    (void)err;
+    const int m = cyclic ? n_row - 1 : n_row;
+    const int nch = (m + CH - 1) / CH;
+    const size_t smem = (size_t)(cyclic ? 3 : 2) * nch * TPB * sizeof(double);
+    if (smem > 200 * 1024) return cudaErrorInvalidConfiguration;
+    dim3 grid((unsigned)(((long)n_sys + TPB - 1) / TPB));
     if (cyclic) {
-        auto kern = k_tdma_arr<true>;
         if (smem > 48 * 1024) {
-            cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            cudaError_t e = cudaFuncSetAttribute(k_thomas_cycl, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             if (e != cudaSuccess) return e;
         }
-        kern<<<grid, threads, smem, st>>>(a, b, c, d, n_sys, n_row, lgS, err);
+        k_thomas_cycl<<<grid, TPB, smem, st>>>(a, b, c, d, n_sys, n_row);
     } else {
-        auto kern = k_tdma_arr<false>;
         if (smem > 48 * 1024) {
-            cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            cudaError_t e = cudaFuncSetAttribute(k_thomas_arr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             if (e != cudaSuccess) return e;
         }
-        kern<<<grid, threads, smem, st>>>(a, b, c, d, n_sys, n_row, lgS, err);
+        k_thomas_arr<<<grid, TPB, smem, st>>>(a, b, c, d, n_sys, n_row);
     }
     return cudaGetLastError();
 }
@@ -455,8 +554,8 @@ __global__ void __launch_bounds__(256) k_zcoef(const double* __restrict__ dx3, c
     double mx = 0.0;
     for (int k = threadIdx.x; k < nz; k += blockDim.x) {
         const int kk = k + 1;
-        double av = 1.0 / dx3[kk] / dmx3[kk];
-        double cv = 1.0 / dx3[kk] / dmx3[kk + 1];
+        double av = __ddiv_rn(__ddiv_rn(1.0, dx3[kk]), dmx3[kk]);
+        double cv = __ddiv_rn(__ddiv_rn(1.0, dx3[kk]), dmx3[kk + 1]);
         if (k == 0) av = 0.0;
         if (k == nz - 1) cv = 0.0;
         am[k] = av;

@@ -266,6 +266,7 @@ __global__ void __launch_bounds__(512) k_yinv(const cx<T>* __restrict__ in, long
                                                Geom g, FftSched sch, int W, int lgW,
                                                const cx<T>* __restrict__ tw_ny,
                                                const cx<T>* __restrict__ tw_dct,
+                                               const double* __restrict__ dc_shift,
                                                const int* __restrict__ skip)
 {
     if (skip && *skip) return;
@@ -275,6 +276,8 @@ __global__ void __launch_bounds__(512) k_yinv(const cx<T>* __restrict__ in, long
     const int z = blockIdx.y;
     const int col0 = blockIdx.x * W;
     const int E = ny << lgW;
+    // the zero mode's z-average, removed from the (kx,ky) = (0,0) coefficient
+    const T shift = (col0 == 0 && dc_shift) ? (T)*dc_shift : (T)0;
 
     if (KIND == Y_C2C) {
         const cx<T>* inp = in + (long)z * ny * in_pitch;
@@ -283,6 +286,7 @@ __global__ void __launch_bounds__(512) k_yinv(const cx<T>* __restrict__ in, long
             const int col = col0 + l;
             cx<T> v = mk<T>((T)0, (T)0);
             if (col < ncols) v = inp[(long)k * in_pitch + col];
+            if (k == 0 && col == 0) v.x -= shift;
             s[sidx<T>(k, l, W)] = v;
         }
     } else if (KIND == Y_CDCT) {
@@ -295,7 +299,8 @@ __global__ void __launch_bounds__(512) k_yinv(const cx<T>* __restrict__ in, long
             const int col = col0 + l;
             cx<T> Z = mk<T>((T)0, (T)0);
             if (col < ncols) {
-                const cx<T> X = inp[(long)k * in_pitch + col];
+                cx<T> X = inp[(long)k * in_pitch + col];
+                if (k == 0 && col == 0) X.x -= shift;
                 const cx<T> Xp = (k == 0) ? mk<T>((T)0, (T)0) : inp[(long)(ny - k) * in_pitch + col];
                 const cx<T> w = ldg(tw_dct + k);
                 const T c = w.x, sn = -w.y;
@@ -318,6 +323,7 @@ __global__ void __launch_bounds__(512) k_yinv(const cx<T>* __restrict__ in, long
                 cx<T> X2 = inp[(long)kk * in_pitch + 2 * col + 1];
                 if (k > ny / 2) { X1 = conj(X1); X2 = conj(X2); }
                 if (k == 0 || k == ny / 2) { X1.y = (T)0; X2.y = (T)0; }
+                if (k == 0 && col == 0) X1.x -= shift;
                 Z = mk<T>(X1.x - X2.y, X1.y + X2.x);
             }
             s[sidx<T>(k, l, W)] = Z;
@@ -344,7 +350,8 @@ __global__ void __launch_bounds__(512) k_yinv(const cx<T>* __restrict__ in, long
 // --------------------------------------------------------------------------
 template <typename T, bool DCT, bool ACC>
 __global__ void __launch_bounds__(512) k_xinv(const void* __restrict__ in_, long in_pitch,
-                                               double* __restrict__ P, Geom g, double* __restrict__ norms,
+                                               double* __restrict__ P, Geom g, double* __restrict__ partials,
+                                               const double* __restrict__ mean_prev,
                                                FftSched sch, int W, int lgW,
                                                const cx<T>* __restrict__ tw_half,
                                                const cx<T>* __restrict__ tw_n,
@@ -392,7 +399,8 @@ __global__ void __launch_bounds__(512) k_xinv(const void* __restrict__ in_, long
     __syncthreads();
     fft_tile<T, true>(s, sch, W, lgW, tw_half);
 
-    double acc_du = 0.0, acc_u = 0.0;
+    double acc_du = 0.0, acc_u = 0.0, acc_s = 0.0;
+    const double mprev = (ACC && mean_prev) ? *mean_prev : 0.0;
     const int Eo = nx << lgW;
     for (int e = threadIdx.x; e < Eo; e += blockDim.x) {
         const int l = e / nx, i = e - l * nx;
@@ -404,24 +412,34 @@ __global__ void __launch_bounds__(512) k_xinv(const void* __restrict__ in_, long
         const double x = (double)((n & 1) ? zv.y : zv.x);
         const int j = (int)(line % g.ny), k = (int)(line / g.ny);
         const long o = (long)(i + 1) + (long)(j + 1) * g.pstride_y + (long)(k + 1) * g.pstride_z;
-        if (ACC) {
-            const double un = P[o] + x;
-            P[o] = un;
+        // refinement: u <- u + du - mean(u), the FP64 mean of the previous
+        // iterate (the residual cannot see constants, so the gauge is kept here)
+        const double un = ACC ? (P[o] - mprev) + x : x;
+        P[o] = un;
+        if (partials) {
             acc_du += x * x;
             acc_u += un * un;
-        } else {
-            P[o] = x;
+            acc_s += un;
         }
     }
-    if (ACC && norms) {
+    if (partials) {
+        // deterministic per-block partial sums (reduced in a fixed order by the gate)
+        __shared__ double red[3][32];
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) {
             acc_du += __shfl_down_sync(0xffffffffu, acc_du, off);
             acc_u += __shfl_down_sync(0xffffffffu, acc_u, off);
+            acc_s += __shfl_down_sync(0xffffffffu, acc_s, off);
         }
-        if ((threadIdx.x & 31) == 0) {
-            atomicAdd(norms + 0, acc_du);
-            atomicAdd(norms + 1, acc_u);
+        const int w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+        if ((threadIdx.x & 31) == 0) { red[0][w] = acc_du; red[1][w] = acc_u; red[2][w] = acc_s; }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double a = 0, b = 0, c = 0;
+            for (int i = 0; i < nw; ++i) { a += red[0][i]; b += red[1][i]; c += red[2][i]; }
+            partials[3 * blockIdx.x + 0] = a;
+            partials[3 * blockIdx.x + 1] = b;
+            partials[3 * blockIdx.x + 2] = c;
         }
     }
 }
@@ -485,7 +503,7 @@ cudaError_t launch_yfwd(int kind, const cx<T>* in, long in_pitch, cx<T>* out, lo
 template <typename T>
 cudaError_t launch_yinv(int kind, const cx<T>* in, long in_pitch, cx<T>* out, long out_pitch, int ncols,
                         const Geom& g, const FftSched& sch, const cx<T>* tw_ny, const cx<T>* tw_dct,
-                        const int* skip_flag, cudaStream_t st)
+                        const double* dc_shift, const int* skip_flag, cudaStream_t st)
 {
     int threads;
     const int W = pick_w<T>(g.ny, threads), lgW = ilog2(W);
@@ -498,7 +516,7 @@ cudaError_t launch_yinv(int kind, const cx<T>* in, long in_pitch, cx<T>* out, lo
         cudaError_t e = set_smem(kern, smem);                                                    \
         if (e != cudaSuccess) return e;                                                          \
         kern<<<grid, threads, smem, st>>>(in, in_pitch, out, out_pitch, ncols, g, sch, W, lgW,  \
-                                         tw_ny, tw_dct, skip_flag);                              \
+                                         tw_ny, tw_dct, dc_shift, skip_flag);                    \
     }
     if (kind == Y_C2C) PPF_YI(Y_C2C)
     else if (kind == Y_CDCT) PPF_YI(Y_CDCT)
@@ -509,8 +527,8 @@ cudaError_t launch_yinv(int kind, const cx<T>* in, long in_pitch, cx<T>* out, lo
 
 template <typename T>
 cudaError_t launch_xinv(bool dct, const void* in, long in_pitch, double* P, const Geom& g, bool accumulate,
-                        double* norms, const FftSched& sch, const cx<T>* tw_half, const cx<T>* tw_n,
-                        const cx<T>* tw_dct, const int* skip_flag, cudaStream_t st)
+                        double* partials, const double* mean_prev, const FftSched& sch, const cx<T>* tw_half,
+                        const cx<T>* tw_n, const cx<T>* tw_dct, const int* skip_flag, cudaStream_t st)
 {
     const int nc = g.nx / 2;
     int threads;
@@ -524,14 +542,25 @@ cudaError_t launch_xinv(bool dct, const void* in, long in_pitch, double* P, cons
         auto kern = k_xinv<T, D, A>;                                                             \
         cudaError_t e = set_smem(kern, smem);                                                    \
         if (e != cudaSuccess) return e;                                                          \
-        kern<<<grid, threads, smem, st>>>(in, in_pitch, P, g, norms, sch, W, lgW, tw_half, tw_n, \
-                                         tw_dct, skip_flag);                                     \
+        kern<<<grid, threads, smem, st>>>(in, in_pitch, P, g, partials, mean_prev, sch, W, lgW,  \
+                                         tw_half, tw_n, tw_dct, skip_flag);                      \
     }
     if (dct) { if (accumulate) PPF_XI(true, true) else PPF_XI(true, false) }
     else     { if (accumulate) PPF_XI(false, true) else PPF_XI(false, false) }
 #undef PPF_XI
     return cudaGetLastError();
 }
+
+template <typename T>
+long xinv_blocks(const Geom& g)
+{
+    int threads;
+    const int W = pick_w<T>(g.nx / 2, threads);
+    const long nlines = (long)g.ny * g.nz;
+    return (nlines + W - 1) / W;
+}
+template long xinv_blocks<double>(const Geom&);
+template long xinv_blocks<float>(const Geom&);
 
 #define PPF_INST(T)                                                                                        \
     template cudaError_t launch_xfwd<T>(bool, const double*, const ResidIn*, const Geom&, void*, long,     \
@@ -541,11 +570,11 @@ cudaError_t launch_xinv(bool dct, const void* in, long in_pitch, double* P, cons
                                         const FftSched&, const cx<T>*, const cx<T>*, const int*,           \
                                         cudaStream_t);                                                     \
     template cudaError_t launch_yinv<T>(int, const cx<T>*, long, cx<T>*, long, int, const Geom&,           \
-                                        const FftSched&, const cx<T>*, const cx<T>*, const int*,           \
-                                        cudaStream_t);                                                     \
+                                        const FftSched&, const cx<T>*, const cx<T>*, const double*,        \
+                                        const int*, cudaStream_t);                                         \
     template cudaError_t launch_xinv<T>(bool, const void*, long, double*, const Geom&, bool, double*,      \
-                                        const FftSched&, const cx<T>*, const cx<T>*, const cx<T>*,         \
-                                        const int*, cudaStream_t);
+                                        const double*, const FftSched&, const cx<T>*, const cx<T>*,        \
+                                        const cx<T>*, const int*, cudaStream_t);
 PPF_INST(double)
 PPF_INST(float)
 #undef PPF_INST

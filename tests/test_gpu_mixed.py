@@ -44,3 +44,20 @@ def test_sweep_gate_stops_early():
     assert 1 <= sweeps < 6 and rel < 1e-9
     R = oracle_solve(p)
     assert rel_l2(P, R) < TOL_MIXED
+
+
+def test_mixed_mean_is_fp64_zero():
+    """The residual cannot see constants; the gauge (zero arithmetic mean) is
+    kept in FP64 by the accumulate pass."""
+    p = W.config3(n1m=128, n2m=128, n3m=64)
+    P = gpu_solve(p, precision=PPF_MIXED, max_sweeps=2)
+    u = P[1:-1, 1:-1, 1:-1]
+    assert abs(u.mean()) < 1e-14 * np.abs(u).max()
+
+
+def test_mixed_deterministic():
+    rng = np.random.default_rng(24)
+    p = W.random_problem(rng, 64, 64, 32, (0, 1, 0), beta=1.0)
+    P1, plan = gpu_solve(p, precision=PPF_MIXED, max_sweeps=2, return_plan=True)
+    P2 = gpu_solve(p, plan=plan)
+    assert np.array_equal(P1, P2)
