@@ -116,6 +116,27 @@ PPF_API int ppf_tdma_many(const double *a, const double *b, const double *c, dou
 PPF_API int ppf_tdma_cycl_many(const double *a, const double *b, const double *c, double *d,
                        int n_sys, int n_row, void *stream);
 
+/* Allocation-free FP64 solve, for callers that cannot allocate device
+ * memory at solve time: a flow solver that reserved its whole device memory
+ * budget at start-up, or an application whose memory is owned by another
+ * framework.  No counterpart in the reference (whose solve allocates its
+ * coefficient arrays on every call).  Same arguments and result as
+ * ppf_plan_create + ppf_solve with precision PPF_FP64, but every work buffer
+ * lives in one static device array of PPF_NOALLOC_SCRATCH_BYTES that each
+ * GPU loading the library holds until the process exits; grids whose work
+ * memory does not fit (about 128^3 cells) are rejected with
+ * PPF_ERR_UNSUPPORTED and a message naming the bytes needed.  The first call
+ * on a device looks up the array's device address; make that first call
+ * before any stream capture.  All calls on a device share the array and it
+ * keeps the last call's contents: calls whose kernels overlap on the GPU
+ * (different streams, or different host threads without ordering) race on
+ * it.  The caller passes inputs and outputs; nothing is allocated, freed or
+ * cached beyond the array itself and a small static host staging table. */
+#define PPF_NOALLOC_SCRATCH_BYTES (64u << 20)
+PPF_API int ppf_solve_noalloc(const ppf_desc *desc, const double *f_d, double *p_d,
+                              const double *dmx1_d, const double *dmx2_d,
+                              const double *dmx3_d, const double *dx3_d, void *stream);
+
 /* Thread-local message describing the last error ("" if none). */
 PPF_API const char *ppf_last_error(void);
 

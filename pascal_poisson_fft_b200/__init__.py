@@ -46,7 +46,7 @@ EXPORTED_SYMBOLS = (
     "ppf_plan_workspace_bytes", "ppf_tdma_many", "ppf_tdma_cycl_many", "ppf_last_error", "ppf_version",
     "ppf_fft_poisson_plan_cuda_create", "ppf_cuda_poisson_fft_initial", "ppf_cuda_poisson_fft_1d",
     "ppf_cuda_poisson_fft_clean", "ppf_cuda_poisson_fft_set_precision", "ppf_stage_timing",
-    "ppf_stage_times",
+    "ppf_stage_times", "ppf_solve_noalloc",
 )
 STAGES = ("z-coefficients", "x-forward", "y-forward", "tdma-z", "y-inverse", "x-inverse",
           "refine-gate", "ghost-cells")
@@ -94,6 +94,7 @@ def lib() -> ctypes.CDLL:
     L.ppf_cuda_poisson_fft_1d.argtypes = [_vp] * 6
     L.ppf_cuda_poisson_fft_set_precision.argtypes = [ctypes.c_int, ctypes.c_int]
     L.ppf_stage_timing.argtypes = [_vp, ctypes.c_int]
+    L.ppf_solve_noalloc.argtypes = [ctypes.POINTER(_Desc)] + [_vp] * 6 + [_vp]
     L.ppf_stage_times.argtypes = [_vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)]
     for name in EXPORTED_SYMBOLS:
         if name not in ("ppf_last_error", "ppf_version"):

@@ -600,3 +600,173 @@ int ppf_tdma_cycl_many(const double* a, const double* b, const double* c, double
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free FP64 solve.  All work memory (spectral buffers, tables,
+// flags) lives in one file-scope device array of PPF_NOALLOC_SCRATCH_BYTES,
+// so the call never allocates device memory.  The array is a per-device
+// global of this library: every call on a device shares it and it keeps the
+// last call's contents; calls whose kernels overlap on the GPU race on it.
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) unsigned char g_noalloc_scratch[PPF_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+
+constexpr int NA_MAXDEV = 64;
+constexpr size_t NA_STAGE = 32768;  // host staging of the tables (doubles)
+
+struct NoallocDev {
+    unsigned char* base = nullptr;  // device address of g_noalloc_scratch on this device
+    bool tables = false;            // tables of `last` are in the array
+    ppf_desc last{};
+};
+
+std::mutex g_na_mu;
+NoallocDev g_na[NA_MAXDEV];
+double g_na_stage[NA_STAGE];
+
+size_t na_align(size_t v) { return (v + 255) & ~(size_t)255; }
+
+bool same_desc(const ppf_desc& a, const ppf_desc& b)
+{
+    return a.n1m == b.n1m && a.n2m == b.n2m && a.n3m == b.n3m && a.L1 == b.L1 && a.L2 == b.L2 &&
+           a.pbc1 == b.pbc1 && a.pbc2 == b.pbc2 && a.pbc3 == b.pbc3;
+}
+
+void na_cexp(int count, long double den, double* out)
+{
+    for (int k = 0; k < count; ++k) {
+        long double a = -2.0L * PI_L * (long double)k / den;
+        out[2 * k] = (double)cosl(a);
+        out[2 * k + 1] = (double)sinl(a);
+    }
+}
+
+}  // namespace
+
+extern "C" int ppf_solve_noalloc(const ppf_desc* desc, const double* f_d, double* p_d, const double* dmx1_d,
+                                 const double* dmx2_d, const double* dmx3_d, const double* dx3_d, void* stream)
+{
+    g_err[0] = 0;
+    std::lock_guard<std::mutex> lk(g_na_mu);
+    int rc = validate(desc);
+    if (rc != PPF_OK) return rc;
+    if (desc->precision != PPF_FP64) return fail(PPF_ERR_UNSUPPORTED, "ppf_solve_noalloc solves in FP64 only");
+    if (!f_d || !p_d || !dmx1_d || !dmx2_d || !dmx3_d || !dx3_d) return fail(PPF_ERR_INVALID, "null array argument");
+    int dev = -1;
+    PPF_CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= NA_MAXDEV) return fail(PPF_ERR_UNSUPPORTED, "device index %d out of range", dev);
+    NoallocDev& nd = g_na[dev];
+    if (!nd.base) {
+        // first call on this device: the device address of the array (the
+        // host-side symbol is not a device address)
+        void* ptr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+        nd.base = static_cast<unsigned char*>(ptr);
+        nd.tables = false;
+    }
+
+    // layout (the same as plan_init's for FP64), carved out of the array
+    ppf_plan p;
+    p.d = *desc;
+    p.d.max_sweeps = 0;
+    p.dev = dev;
+    const int nx = desc->n1m, ny = desc->n2m, nz = desc->n3m;
+    p.g.nx = nx; p.g.ny = ny; p.g.nz = nz;
+    p.g.px = desc->pbc1 ? 1 : 0; p.g.py = desc->pbc2 ? 1 : 0; p.g.pz = desc->pbc3 ? 1 : 0;
+    p.g.pstride_y = nx + 2;
+    p.g.pstride_z = (long)(nx + 2) * (ny + 2);
+    p.xdct = !desc->pbc1;
+    p.ydct = !desc->pbc2;
+    p.elem = 8;
+    factor(nx / 2, p.sx);
+    factor(ny, p.sy);
+    const size_t ce = 16;
+    const int nh = nx / 2 + 1;
+    if (!p.xdct) {
+        p.a_pitch = round_up(nh, 16);
+        p.a_bytes = (size_t)p.a_pitch * ny * nz * ce;
+        p.ycols = nh;
+        p.b_pitch = p.a_pitch;
+        p.ykind = p.ydct ? Y_CDCT : Y_C2C;
+        p.mx = nh; p.my = ny;
+        p.b_bytes = (size_t)p.b_pitch * ny * nz * ce;
+        p.cplx = true;
+    } else {
+        p.a_pitch = round_up(nx, 32);
+        p.a_bytes = (size_t)p.a_pitch * ny * nz * 8;
+        p.ycols = nx / 2;
+        if (p.ydct) {
+            p.ykind = Y_CDCT; p.b_pitch = p.a_pitch; p.mx = nx; p.my = ny;
+            p.b_bytes = (size_t)p.b_pitch * ny * nz * 8;
+            p.cplx = false;
+        } else {
+            p.ykind = Y_RPAIR; p.b_pitch = round_up(nx, 16); p.mx = nx; p.my = ny / 2 + 1;
+            p.b_bytes = (size_t)p.b_pitch * (ny / 2 + 1) * nz * ce;
+            p.cplx = true;
+        }
+    }
+    p.scale = 1.0 / ((p.xdct ? 2.0 * nx : (double)nx) * (p.ydct ? 2.0 * ny : (double)ny));
+    // twiddle parts as upload_twiddles<double> lays them out
+    const int tw_cnt[5] = { nx / 2, nx, nx, ny, ny };
+    size_t tw_doubles = 0;
+    for (int i = 0; i < 5; ++i) {
+        p.tw_off[i] = tw_doubles / 2;
+        tw_doubles += 2 * (size_t)tw_cnt[i];
+        while (tw_doubles % 4) ++tw_doubles;
+    }
+    size_t off = 0;
+    const size_t oA = off; off = na_align(off + p.a_bytes);
+    const size_t oB = off; off = na_align(off + p.b_bytes);
+    const size_t oLx = off; off = na_align(off + sizeof(double) * p.mx);
+    const size_t oLy = off; off = na_align(off + sizeof(double) * p.my);
+    const size_t oAm = off; off = na_align(off + sizeof(double) * nz);
+    const size_t oAp = off; off = na_align(off + sizeof(double) * nz);
+    const size_t oSc = off; off = na_align(off + sizeof(double) * 8);
+    const size_t oFl = off; off = na_align(off + sizeof(int) * 4);
+    const size_t oTw = off; off = na_align(off + sizeof(double) * tw_doubles);
+    if (off > (size_t)PPF_NOALLOC_SCRATCH_BYTES)
+        return fail(PPF_ERR_UNSUPPORTED,
+                    "grid %dx%dx%d needs %zu bytes of work memory; ppf_solve_noalloc holds %zu (use ppf_plan_create)",
+                    nx, ny, nz, off, (size_t)PPF_NOALLOC_SCRATCH_BYTES);
+    if ((size_t)(p.mx + p.my) + tw_doubles > NA_STAGE)
+        return fail(PPF_ERR_UNSUPPORTED, "table staging for %dx%d exceeds %zu values", nx, ny, NA_STAGE);
+    unsigned char* b = nd.base;
+    p.A = b + oA; p.B = b + oB;
+    p.lamx = reinterpret_cast<double*>(b + oLx);
+    p.lamy = reinterpret_cast<double*>(b + oLy);
+    p.am = reinterpret_cast<double*>(b + oAm);
+    p.ap = reinterpret_cast<double*>(b + oAp);
+    p.scal = reinterpret_cast<double*>(b + oSc);
+    p.flags = reinterpret_cast<int*>(b + oFl);
+    p.tw = b + oTw;
+
+    cudaStream_t st = (cudaStream_t)stream;
+    if (!nd.tables || !same_desc(nd.last, *desc)) {
+        // wavenumbers and twiddles, computed as plan_init does, staged in a
+        // static host array (pageable copies return once the data is staged)
+        double* lx = g_na_stage;
+        double* ly = lx + p.mx;
+        const double hx = desc->L1 / nx, hy = desc->L2 / ny;
+        for (int i = 0; i < p.mx; ++i) lx[i] = p.xdct ? wn_dct(i, nx, hx) : wn_fft(i, nx, hx);
+        for (int j = 0; j < p.my; ++j) {
+            if (p.ydct) { ly[j] = wn_dct(j, ny, hy); continue; }
+            int jm = j;
+            if (!p.xdct && j + 1 > ny / 2 + 1) jm = ny - j;
+            ly[j] = wn_fft(jm, ny, hy);
+        }
+        double* tw = ly + p.my;
+        for (size_t q = 0; q < tw_doubles; ++q) tw[q] = 0.0;
+        const long double den[5] = { (long double)(nx / 2), (long double)nx, 4.0L * nx, (long double)ny, 4.0L * ny };
+        for (int i = 0; i < 5; ++i) na_cexp(tw_cnt[i], den[i], tw + 2 * p.tw_off[i]);
+        nd.tables = false;
+        PPF_CK(cudaMemcpyAsync(p.lamx, lx, sizeof(double) * p.mx, cudaMemcpyHostToDevice, st));
+        PPF_CK(cudaMemcpyAsync(p.lamy, ly, sizeof(double) * p.my, cudaMemcpyHostToDevice, st));
+        PPF_CK(cudaMemcpyAsync(p.tw, tw, sizeof(double) * tw_doubles, cudaMemcpyHostToDevice, st));
+        nd.last = *desc;
+        nd.tables = true;
+    }
+    PPF_CK(cudaMemsetAsync(p.scal, 0, sizeof(double) * 8, st));
+    return solve_impl(&p, f_d, p_d, dmx1_d, dmx2_d, dmx3_d, dx3_d, st);
+}
