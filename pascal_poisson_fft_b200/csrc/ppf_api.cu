@@ -107,6 +107,7 @@ struct ppf_plan {
     int* flags = nullptr;      // [0] skip, [1] sweeps_done, [2] err
     double* partials = nullptr;  // per-block sums of the x-inverse pass (mixed precision)
     long xinv_nblk = 0;
+    double* ckpt = nullptr;      // Thomas checkpoints of the z solve
     void* tw = nullptr;        // twiddle tables (type T)
     size_t tw_off[5] = {};     // element offsets: x half, x n, x dct, y n, y dct
     FftSched sx{}, sy{};
@@ -167,7 +168,7 @@ void free_plan(ppf_plan* p)
     if (!p) return;
     drop_marks(p);
     void* ptrs[] = { p->A, p->B, p->lamx, p->lamy, p->am, p->ap, p->scal, p->flags, p->tw,
-                     p->f_dev, p->p_dev, p->m_dev, p->partials };
+                     p->f_dev, p->p_dev, p->m_dev, p->partials, p->ckpt };
     for (void* q : ptrs)
         if (q) cudaFree(q);
     delete p;
@@ -274,6 +275,7 @@ int plan_init(ppf_plan* p, const ppf_desc* d)
         p->xinv_nblk = xinv_blocks<float>(p->g);
         PPF_CK(cudaMalloc(&p->partials, sizeof(double) * 3 * p->xinv_nblk));
     }
+    PPF_CK(cudaMalloc(&p->ckpt, sizeof(double) * tdma_z_ckpt_doubles(nz, p->b_pitch * (long)p->my, p->g.pz)));
     PPF_CK(cudaMemcpy(p->lamx, lx.data(), sizeof(double) * p->mx, cudaMemcpyHostToDevice));
     PPF_CK(cudaMemcpy(p->lamy, ly.data(), sizeof(double) * p->my, cudaMemcpyHostToDevice));
     int rc = (p->elem == 8) ? upload_twiddles<double>(p) : upload_twiddles<float>(p);
@@ -317,6 +319,7 @@ int run_pass(ppf_plan* p, const double* f, double* P, bool resid, bool accumulat
     z.dzmax2 = p->scal;
     z.dc_shift = p->scal + 4;
     z.cyclic = p->g.pz;
+    z.ckpt = p->ckpt;
     e = p->cplx ? launch_tdma_z<T, true>(p->B, z, skip, p->flags + 2, st)
                 : launch_tdma_z<T, false>(p->B, z, skip, p->flags + 2, st);
     if (e != cudaSuccess) return cuda_fail(e, "z tridiagonal");
@@ -726,6 +729,7 @@ extern "C" int ppf_solve_noalloc(const ppf_desc* desc, const double* f_d, double
     const size_t oSc = off; off = na_align(off + sizeof(double) * 8);
     const size_t oFl = off; off = na_align(off + sizeof(int) * 4);
     const size_t oTw = off; off = na_align(off + sizeof(double) * tw_doubles);
+    const size_t oCk = off; off = na_align(off + sizeof(double) * tdma_z_ckpt_doubles(nz, p.b_pitch * (long)p.my, p.g.pz));
     if (off > (size_t)PPF_NOALLOC_SCRATCH_BYTES)
         return fail(PPF_ERR_UNSUPPORTED,
                     "grid %dx%dx%d needs %zu bytes of work memory; ppf_solve_noalloc holds %zu (use ppf_plan_create)",
@@ -741,6 +745,7 @@ extern "C" int ppf_solve_noalloc(const ppf_desc* desc, const double* f_d, double
     p.scal = reinterpret_cast<double*>(b + oSc);
     p.flags = reinterpret_cast<int*>(b + oFl);
     p.tw = b + oTw;
+    p.ckpt = reinterpret_cast<double*>(b + oCk);
 
     cudaStream_t st = (cudaStream_t)stream;
     if (!nd.tables || !same_desc(nd.last, *desc)) {
@@ -768,5 +773,7 @@ extern "C" int ppf_solve_noalloc(const ppf_desc* desc, const double* f_d, double
         nd.tables = true;
     }
     PPF_CK(cudaMemsetAsync(p.scal, 0, sizeof(double) * 8, st));
-    return solve_impl(&p, f_d, p_d, dmx1_d, dmx2_d, dmx3_d, dx3_d, st);
+    rc = solve_impl(&p, f_d, p_d, dmx1_d, dmx2_d, dmx3_d, dx3_d, st);
+    p.ckpt = nullptr;
+    return rc;
 }

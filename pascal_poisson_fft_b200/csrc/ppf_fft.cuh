@@ -221,4 +221,85 @@ __device__ __forceinline__ void fft_tile(cx<T>* s, const FftSched& sch, int W, i
     }
 }
 
+// ---------------------------------------------------------------------------
+// Compile-time engine: length N, W lines, NT threads and the radix sequence
+// are template parameters, so every index, division and loop bound is a
+// constant.  Same layout and pass structure as fft_tile.
+// ---------------------------------------------------------------------------
+template <typename T, int W>
+__device__ __forceinline__ int sidx_ct(int n, int l)
+{
+    constexpr int G = SwizzleG<T>::value;
+    constexpr int MASK = (W < G ? W : G) - 1;
+    return n * W + (l ^ (n & MASK));
+}
+
+template <typename T, bool INV, int N, int W, int NT, int R, int NS>
+__device__ __forceinline__ void fft_pass_ct(cx<T>* s, const cx<T>* __restrict__ tw)
+{
+    constexpr int NB = N / R;
+    constexpr int ITEMS = NB * W;
+    constexpr int Q = (ITEMS + NT - 1) / NT;
+    constexpr int TS = N / (NS * R);
+    cx<T> v[Q * R];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        const int t = threadIdx.x + q * NT;
+        if (ITEMS % NT == 0 || t < ITEMS) {
+            const int l = t % W, j = t / W;
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[q * R + r] = s[sidx_ct<T, W>(j + r * NB, l)];
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        const int t = threadIdx.x + q * NT;
+        if (ITEMS % NT == 0 || t < ITEMS) {
+            const int l = t % W, j = t / W;
+            const int k = j % NS;
+            if (NS > 1) {
+#pragma unroll
+                for (int r = 1; r < R; ++r) {
+                    cx<T> w = ldg(tw + r * k * TS);
+                    if (INV) w.y = -w.y;
+                    v[q * R + r] = cmul(v[q * R + r], w);
+                }
+            }
+            Dft<T, INV, R>::run(v + q * R);
+            const int base = (j - k) * R + k;
+#pragma unroll
+            for (int r = 0; r < R; ++r) s[sidx_ct<T, W>(base + r * NS, l)] = v[q * R + r];
+        }
+    }
+    __syncthreads();
+}
+
+template <typename T, bool INV, int N, int W, int NT, int NS>
+__device__ __forceinline__ void fft_ct_passes(cx<T>*, const cx<T>* __restrict__) {}
+
+template <typename T, bool INV, int N, int W, int NT, int NS, int R0, int... RS>
+__device__ __forceinline__ void fft_ct_passes(cx<T>* s, const cx<T>* __restrict__ tw)
+{
+    fft_pass_ct<T, INV, N, W, NT, R0, NS>(s, tw);
+    fft_ct_passes<T, INV, N, W, NT, NS * R0, RS...>(s, tw);
+}
+
+// Tile shapes.  ShapeRT: everything at run time (fft_tile).  ShapeCT: a
+// fixed length N = product of RS, W lines, NT threads per CTA.
+struct ShapeRT {
+    static constexpr bool CT = false;
+    static constexpr int N = 0, W = 0, NT = 0;
+};
+template <int N_, int W_, int NT_, int... RS>
+struct ShapeCT {
+    static constexpr bool CT = true;
+    static constexpr int N = N_, W = W_, NT = NT_;
+    template <typename T, bool INV>
+    static __device__ __forceinline__ void fft(cx<T>* s, const cx<T>* __restrict__ tw)
+    {
+        fft_ct_passes<T, INV, N_, W_, NT_, 1, RS...>(s, tw);
+    }
+};
+
 }  // namespace ppf

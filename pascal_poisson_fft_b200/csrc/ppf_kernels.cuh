@@ -73,7 +73,11 @@ struct ZSys {
     const double* dzmax2; // device scalar: max_k dx3_k^2 (written by the z-coefficient kernel)
     double* dc_shift;     // device scalar: z-average of the (0,0) solution (subtracted by the y inverse)
     int cyclic;           // periodic z: the reference's cyclic Thomas sequence
+    double* ckpt;         // Thomas checkpoints, tdma_z_ckpt_doubles(nz, plane, cyclic) doubles
 };
+
+// doubles of checkpoint memory the z solve needs
+long tdma_z_ckpt_doubles(int nz, long plane, int cyclic);
 
 template <typename T, bool CPLX>
 cudaError_t launch_tdma_z(void* data, const ZSys& z, const int* skip_flag, int* err_flag, cudaStream_t st);

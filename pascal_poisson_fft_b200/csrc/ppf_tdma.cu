@@ -42,21 +42,6 @@ namespace {
 constexpr int CH = 16;  // rows per checkpoint chunk
 constexpr int TPB = 128;
 
-// explicitly rounded arithmetic (no FMA contraction) in type CT
-template <typename CT> struct R;
-template <> struct R<double> {
-    static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
-    static __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
-    static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
-    static __device__ __forceinline__ double div(double a, double b) { return __ddiv_rn(a, b); }
-};
-template <> struct R<float> {
-    static __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
-    static __device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
-    static __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
-    static __device__ __forceinline__ float div(float a, float b) { return __fdiv_rn(a, b); }
-};
-
 template <typename T, bool CPLX> struct Elem;
 template <typename T> struct Elem<T, true> { using type = cx<T>; };
 template <typename T> struct Elem<T, false> { using type = T; };
@@ -81,113 +66,156 @@ template <typename T> __device__ __forceinline__ void st_elem(T* p, double r, do
     *p = (T)r;
 }
 
-// Poisson coefficients of row zr (a, b, c) in CT.
+// Poisson coefficient sources of one system (see coef_row).
 struct Coef {
     const double* am;
     const double* ap;
     double lx, ly;
     bool pin;
-    template <typename CT>
-    __device__ __forceinline__ void get(int zr, CT& a, CT& b, CT& c) const
-    {
-        if (pin && zr == 0) {
-            a = (CT)0; b = (CT)1; c = (CT)0;
-            return;
-        }
-        const double amv = __ldg(am + zr), apv = __ldg(ap + zr);
-        a = (CT)amv;
-        c = (CT)apv;
-        // b = ac - dxk2 - dyk2 with ac = -am - ap, left to right, in CT
-        b = R<CT>::sub(R<CT>::sub(R<CT>::sub((CT)(-amv), (CT)apv), (CT)lx), (CT)ly);
-    }
 };
 
-// One Thomas forward step on row state (c', d'): first row (zr == 0) divides.
-template <typename CT, bool CPLX>
-__device__ __forceinline__ void fwd_row(bool first, CT a, CT b, CT c, CT dr_in, CT di_in, CT& cp, CT& dr, CT& di)
+// Arithmetic policies: Exact reproduces the reference's rounding (FP64,
+// explicitly rounded intrinsics, IEEE division); Fast is the FP32 path of
+// the mixed-precision solve (its error is removed by the FP64 refinement),
+// free to contract and to use the approximate reciprocal.
+struct Exact {
+    using T = double;
+    static constexpr int CH = 8;    // rows per checkpoint chunk (register budget of FP64 complex rows)
+    static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+    static __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+    static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+    static __device__ __forceinline__ double div(double a, double b) { return __ddiv_rn(a, b); }
+    static __device__ __forceinline__ double rcp(double a) { return __drcp_rn(a); }   // == 1.0/a, correctly rounded
+};
+struct Fast {
+    using T = float;
+    static constexpr int CH = 8;
+    static __device__ __forceinline__ float mul(float a, float b) { return a * b; }
+    static __device__ __forceinline__ float sub(float a, float b) { return a - b; }
+    static __device__ __forceinline__ float add(float a, float b) { return a + b; }
+    static __device__ __forceinline__ float div(float a, float b) { return __fdividef(a, b); }
+    static __device__ __forceinline__ float rcp(float a) { return __fdividef(1.0f, a); }
+};
+
+// b = ac - dxk2 - dyk2 with ac = -am - ap, left to right
+template <typename A>
+__device__ __forceinline__ void coef_row(const Coef& co, int zr, typename A::T& a, typename A::T& b,
+                                         typename A::T& c)
+{
+    using CT = typename A::T;
+    if (co.pin && zr == 0) {
+        a = (CT)0; b = (CT)1; c = (CT)0;
+        return;
+    }
+    const double amv = __ldg(co.am + zr), apv = __ldg(co.ap + zr);
+    a = (CT)amv;
+    c = (CT)apv;
+    b = A::sub(A::sub(A::sub((CT)(-amv), (CT)apv), (CT)co.lx), (CT)co.ly);
+}
+
+// One Thomas forward step on the row state (c', d'); the first row divides.
+template <typename A, bool CPLX>
+__device__ __forceinline__ void fwd_row(bool first, typename A::T a, typename A::T b, typename A::T c,
+                                        typename A::T dr_in, typename A::T di_in, typename A::T& cp,
+                                        typename A::T& dr, typename A::T& di)
 {
     if (first) {
-        dr = R<CT>::div(dr_in, b);
-        if (CPLX) di = R<CT>::div(di_in, b);
-        cp = R<CT>::div(c, b);
+        dr = A::div(dr_in, b);
+        if (CPLX) di = A::div(di_in, b);
+        cp = A::div(c, b);
     } else {
-        const CT r = R<CT>::div((CT)1, R<CT>::sub(b, R<CT>::mul(a, cp)));
-        dr = R<CT>::mul(r, R<CT>::sub(dr_in, R<CT>::mul(a, dr)));
-        if (CPLX) di = R<CT>::mul(r, R<CT>::sub(di_in, R<CT>::mul(a, di)));
-        cp = R<CT>::mul(r, c);
+        const typename A::T r = A::rcp(A::sub(b, A::mul(a, cp)));
+        dr = A::mul(r, A::sub(dr_in, A::mul(a, dr)));
+        if (CPLX) di = A::mul(r, A::sub(di_in, A::mul(a, di)));
+        cp = A::mul(r, c);
     }
 }
 
-// The whole z-solve of one Poisson system in arithmetic type CT.
-// ck: this thread's checkpoint column (stride TPB), 3 values per chunk.
-template <typename T, typename CT, bool CPLX>
+template <typename T, typename CT>
+__device__ __forceinline__ void ld_cv(const cx<T>* p, CT& r, CT& i)
+{
+    const cx<T> v = *p;
+    r = (CT)v.x;
+    i = (CT)v.y;
+}
+template <typename T, typename CT>
+__device__ __forceinline__ void ld_cv(const T* p, CT& r, CT& i)
+{
+    r = (CT)*p;
+    i = (CT)0;
+}
+
+// The z-solve of one Poisson system.  Checkpoints (c', d'r, d'i) after
+// every CH rows go to global memory, [chunk][component][system], so each
+// warp's checkpoint traffic is coalesced and the shared memory stays free.
+template <typename T, typename A, bool CPLX>
 __device__ __forceinline__ void thomas_poisson(typename Elem<T, CPLX>::type* data, long sys, long plane, int nz,
                                                const Coef& co, double scale, double* ck, double& zsum, bool& bad)
 {
+    using CT = typename A::T;
+    constexpr int CH = A::CH;
     const int nch = (nz + CH - 1) / CH;
     CT cp = 0, dr = 0, di = 0;
-    // forward sweep
     for (int ch = 0; ch < nch; ++ch) {
         const int z0 = ch * CH;
-        double vr[CH], vi[CH];
+        CT vr[CH], vi[CH];
 #pragma unroll
         for (int r = 0; r < CH; ++r) {
-            vr[r] = 0.0; vi[r] = 0.0;
-            if (z0 + r < nz) ld_elem<T>(data + (long)(z0 + r) * plane + sys, vr[r], vi[r]);
+            vr[r] = (CT)0; vi[r] = (CT)0;
+            if (z0 + r < nz) ld_cv<T, CT>(data + (long)(z0 + r) * plane + sys, vr[r], vi[r]);
         }
 #pragma unroll
         for (int r = 0; r < CH; ++r) {
             const int zr = z0 + r;
             if (zr < nz) {
                 CT a, b, c;
-                co.get<CT>(zr, a, b, c);
+                coef_row<A>(co, zr, a, b, c);
                 const bool pinrow = co.pin && zr == 0;
-                fwd_row<CT, CPLX>(zr == 0, a, b, c, pinrow ? (CT)0 : (CT)vr[r], pinrow ? (CT)0 : (CT)vi[r], cp, dr, di);
+                fwd_row<A, CPLX>(zr == 0, a, b, c, pinrow ? (CT)0 : vr[r], pinrow ? (CT)0 : vi[r], cp, dr, di);
             }
         }
-        ck[(3 * ch + 0) * TPB] = (double)cp;
-        ck[(3 * ch + 1) * TPB] = (double)dr;
-        ck[(3 * ch + 2) * TPB] = (double)di;
+        double* c3 = ck + (long)(3 * ch) * plane;
+        c3[0] = (double)cp;
+        c3[plane] = (double)dr;
+        if (CPLX) c3[2 * plane] = (double)di;
     }
-    // backward sweep, chunk by chunk from the top
     CT xr = 0, xi = 0;
     for (int ch = nch - 1; ch >= 0; --ch) {
         const int z0 = ch * CH;
-        CT c_[CH], r_[CH], i_[CH];
-        double vr[CH], vi[CH];
+        CT vr[CH], vi[CH], c_[CH];
 #pragma unroll
         for (int r = 0; r < CH; ++r) {
-            vr[r] = 0.0; vi[r] = 0.0;
-            if (z0 + r < nz) ld_elem<T>(data + (long)(z0 + r) * plane + sys, vr[r], vi[r]);
+            vr[r] = (CT)0; vi[r] = (CT)0;
+            if (z0 + r < nz) ld_cv<T, CT>(data + (long)(z0 + r) * plane + sys, vr[r], vi[r]);
         }
         CT pcp = 0, pdr = 0, pdi = 0;
         if (ch > 0) {
-            pcp = (CT)ck[(3 * (ch - 1) + 0) * TPB];
-            pdr = (CT)ck[(3 * (ch - 1) + 1) * TPB];
-            pdi = (CT)ck[(3 * (ch - 1) + 2) * TPB];
+            const double* c3 = ck + (long)(3 * (ch - 1)) * plane;
+            pcp = (CT)c3[0];
+            pdr = (CT)c3[plane];
+            if (CPLX) pdi = (CT)c3[2 * plane];
         }
 #pragma unroll
         for (int r = 0; r < CH; ++r) {
             const int zr = z0 + r;
             if (zr < nz) {
                 CT a, b, c;
-                co.get<CT>(zr, a, b, c);
+                coef_row<A>(co, zr, a, b, c);
                 const bool pinrow = co.pin && zr == 0;
-                fwd_row<CT, CPLX>(zr == 0, a, b, c, pinrow ? (CT)0 : (CT)vr[r], pinrow ? (CT)0 : (CT)vi[r], pcp, pdr,
-                                  pdi);
+                fwd_row<A, CPLX>(zr == 0, a, b, c, pinrow ? (CT)0 : vr[r], pinrow ? (CT)0 : vi[r], pcp, pdr, pdi);
             }
-            c_[r] = pcp; r_[r] = pdr; i_[r] = pdi;
+            c_[r] = pcp; vr[r] = pdr; vi[r] = pdi;
         }
 #pragma unroll
         for (int r = CH - 1; r >= 0; --r) {
             const int zr = z0 + r;
             if (zr < nz) {
                 if (zr == nz - 1) {
-                    xr = r_[r];
-                    xi = i_[r];
+                    xr = vr[r];
+                    xi = vi[r];
                 } else {
-                    xr = R<CT>::sub(r_[r], R<CT>::mul(c_[r], xr));
-                    if (CPLX) xi = R<CT>::sub(i_[r], R<CT>::mul(c_[r], xi));
+                    xr = A::sub(vr[r], A::mul(c_[r], xr));
+                    if (CPLX) xi = A::sub(vi[r], A::mul(c_[r], xi));
                 }
                 const double sr = (double)xr * scale, si = (double)xi * scale;
                 zsum += sr;
@@ -205,97 +233,97 @@ __device__ __forceinline__ void thomas_poisson(typename Elem<T, CPLX>::type* dat
 // rows 1..nz-1 are swept for d and e (e_1 = -a_1, e_{nz-1} = -c_{nz-1}),
 // x_0 is formed from the back-substituted d_1, e_1, then x_i = d_i + x_0 e_i.
 // The back substitution runs twice (first for d_1, e_1) instead of storing e.
-template <typename T, typename CT, bool CPLX>
+template <typename T, typename A, bool CPLX>
 __device__ __forceinline__ void thomas_poisson_cyc(typename Elem<T, CPLX>::type* data, long sys, long plane, int nz,
                                                    const Coef& co, double scale, double* ck, double& zsum, bool& bad)
 {
+    using CT = typename A::T;
+    constexpr int CH = A::CH;
     const int m = nz - 1;
     const int nch = (m + CH - 1) / CH;
     CT a1, b1, c1, an, bn, cn;
-    co.get<CT>(1, a1, b1, c1);
-    co.get<CT>(nz - 1, an, bn, cn);
+    coef_row<A>(co, 1, a1, b1, c1);
+    coef_row<A>(co, nz - 1, an, bn, cn);
     const CT e_first = -a1, e_last = -cn;
     auto e_in = [&](int q) -> CT { return (q == m - 1) ? e_last : ((q == 0) ? e_first : (CT)0); };
     CT cp = 0, dr = 0, di = 0, ep = 0, dum = 0;
     for (int ch = 0; ch < nch; ++ch) {
         const int q0 = ch * CH;
-        double vr[CH], vi[CH];
+        CT vr[CH], vi[CH];
 #pragma unroll
         for (int r = 0; r < CH; ++r) {
-            vr[r] = 0.0; vi[r] = 0.0;
-            if (q0 + r < m) ld_elem<T>(data + (long)(q0 + r + 1) * plane + sys, vr[r], vi[r]);
+            vr[r] = (CT)0; vi[r] = (CT)0;
+            if (q0 + r < m) ld_cv<T, CT>(data + (long)(q0 + r + 1) * plane + sys, vr[r], vi[r]);
         }
 #pragma unroll
         for (int r = 0; r < CH; ++r) {
             const int q = q0 + r;
             if (q < m) {
                 CT a, b, c;
-                co.get<CT>(q + 1, a, b, c);
+                coef_row<A>(co, q + 1, a, b, c);
                 CT cpe = cp;
-                fwd_row<CT, CPLX>(q == 0, a, b, c, (CT)vr[r], (CT)vi[r], cp, dr, di);
-                fwd_row<CT, false>(q == 0, a, b, c, e_in(q), (CT)0, cpe, ep, dum);
+                fwd_row<A, CPLX>(q == 0, a, b, c, vr[r], vi[r], cp, dr, di);
+                fwd_row<A, false>(q == 0, a, b, c, e_in(q), (CT)0, cpe, ep, dum);
             }
         }
-        ck[(4 * ch + 0) * TPB] = (double)cp;
-        ck[(4 * ch + 1) * TPB] = (double)dr;
-        ck[(4 * ch + 2) * TPB] = (double)di;
-        ck[(4 * ch + 3) * TPB] = (double)ep;
+        double* c4 = ck + (long)(4 * ch) * plane;
+        c4[0] = (double)cp;
+        c4[plane] = (double)dr;
+        c4[2 * plane] = (double)di;
+        c4[3 * plane] = (double)ep;
     }
     const CT dtop_r = dr, dtop_i = di, etop = ep;
     CT d1r = 0, d1i = 0, e1 = 0;
-    double x0r = 0.0, x0i = 0.0;
+    CT x0r = 0, x0i = 0;
     for (int pass = 0; pass < 2; ++pass) {
         if (pass == 1) {
             CT a0, b0, c0;
-            co.get<CT>(0, a0, b0, c0);
-            double v0r = 0.0, v0i = 0.0;
-            if (!(co.pin)) ld_elem<T>(data + sys, v0r, v0i);
-            const CT den = R<CT>::add(R<CT>::add(b0, R<CT>::mul(a0, etop)), R<CT>::mul(c0, e1));
-            x0r = (double)R<CT>::div(R<CT>::sub(R<CT>::sub((CT)v0r, R<CT>::mul(a0, dtop_r)), R<CT>::mul(c0, d1r)), den);
-            x0i = (double)R<CT>::div(R<CT>::sub(R<CT>::sub((CT)v0i, R<CT>::mul(a0, dtop_i)), R<CT>::mul(c0, d1i)), den);
+            coef_row<A>(co, 0, a0, b0, c0);
+            CT v0r = 0, v0i = 0;
+            if (!co.pin) ld_cv<T, CT>(data + sys, v0r, v0i);
+            const CT den = A::add(A::add(b0, A::mul(a0, etop)), A::mul(c0, e1));
+            x0r = A::div(A::sub(A::sub(v0r, A::mul(a0, dtop_r)), A::mul(c0, d1r)), den);
+            x0i = A::div(A::sub(A::sub(v0i, A::mul(a0, dtop_i)), A::mul(c0, d1i)), den);
         }
         CT yr = 0, yi = 0, ye = 0;
         for (int ch = nch - 1; ch >= 0; --ch) {
             const int q0 = ch * CH;
-            double vr[CH], vi[CH];
+            CT vr[CH], vi[CH], c_[CH], e_[CH];
 #pragma unroll
             for (int r = 0; r < CH; ++r) {
-                vr[r] = 0.0; vi[r] = 0.0;
-                if (q0 + r < m) ld_elem<T>(data + (long)(q0 + r + 1) * plane + sys, vr[r], vi[r]);
+                vr[r] = (CT)0; vi[r] = (CT)0;
+                if (q0 + r < m) ld_cv<T, CT>(data + (long)(q0 + r + 1) * plane + sys, vr[r], vi[r]);
             }
             CT pc = 0, pr = 0, pi = 0, pe = 0;
             if (ch > 0) {
-                pc = (CT)ck[(4 * (ch - 1) + 0) * TPB];
-                pr = (CT)ck[(4 * (ch - 1) + 1) * TPB];
-                pi = (CT)ck[(4 * (ch - 1) + 2) * TPB];
-                pe = (CT)ck[(4 * (ch - 1) + 3) * TPB];
+                const double* c4 = ck + (long)(4 * (ch - 1)) * plane;
+                pc = (CT)c4[0]; pr = (CT)c4[plane]; pi = (CT)c4[2 * plane]; pe = (CT)c4[3 * plane];
             }
-            CT c_[CH], r_[CH], i_[CH], e_[CH];
 #pragma unroll
             for (int r = 0; r < CH; ++r) {
                 const int q = q0 + r;
                 if (q < m) {
                     CT a, b, c;
-                    co.get<CT>(q + 1, a, b, c);
+                    coef_row<A>(co, q + 1, a, b, c);
                     CT pce = pc;
-                    fwd_row<CT, CPLX>(q == 0, a, b, c, (CT)vr[r], (CT)vi[r], pc, pr, pi);
-                    fwd_row<CT, false>(q == 0, a, b, c, e_in(q), (CT)0, pce, pe, dum);
+                    fwd_row<A, CPLX>(q == 0, a, b, c, vr[r], vi[r], pc, pr, pi);
+                    fwd_row<A, false>(q == 0, a, b, c, e_in(q), (CT)0, pce, pe, dum);
                 }
-                c_[r] = pc; r_[r] = pr; i_[r] = pi; e_[r] = pe;
+                c_[r] = pc; vr[r] = pr; vi[r] = pi; e_[r] = pe;
             }
 #pragma unroll
             for (int r = CH - 1; r >= 0; --r) {
                 const int q = q0 + r;
                 if (q < m) {
-                    if (q == m - 1) { yr = r_[r]; yi = i_[r]; ye = e_[r]; }
+                    if (q == m - 1) { yr = vr[r]; yi = vi[r]; ye = e_[r]; }
                     else {
-                        yr = R<CT>::sub(r_[r], R<CT>::mul(c_[r], yr));
-                        if (CPLX) yi = R<CT>::sub(i_[r], R<CT>::mul(c_[r], yi));
-                        ye = R<CT>::sub(e_[r], R<CT>::mul(c_[r], ye));
+                        yr = A::sub(vr[r], A::mul(c_[r], yr));
+                        if (CPLX) yi = A::sub(vi[r], A::mul(c_[r], yi));
+                        ye = A::sub(e_[r], A::mul(c_[r], ye));
                     }
                     if (pass == 1) {
-                        const CT xr = R<CT>::add(yr, R<CT>::mul((CT)x0r, ye));
-                        const CT xi = CPLX ? R<CT>::add(yi, R<CT>::mul((CT)x0i, ye)) : (CT)0;
+                        const CT xr = A::add(yr, A::mul(x0r, ye));
+                        const CT xi = CPLX ? A::add(yi, A::mul(x0i, ye)) : (CT)0;
                         const double sr = (double)xr * scale, si = (double)xi * scale;
                         zsum += sr;
                         if (!isfinite(sr) || !isfinite(si)) bad = true;
@@ -306,7 +334,7 @@ __device__ __forceinline__ void thomas_poisson_cyc(typename Elem<T, CPLX>::type*
         }
         if (pass == 0) { d1r = yr; d1i = yi; e1 = ye; }
     }
-    const double sr = x0r * scale, si = x0i * scale;
+    const double sr = (double)x0r * scale, si = (double)x0i * scale;
     zsum += sr;
     if (!isfinite(sr) || !isfinite(si)) bad = true;
     st_elem<T>(data + sys, sr, si);
@@ -314,52 +342,66 @@ __device__ __forceinline__ void thomas_poisson_cyc(typename Elem<T, CPLX>::type*
 
 }  // namespace
 
-template <typename T, bool CPLX>
+// MODE 0: every system, arithmetic A.  MODE 1: only systems above the
+// low-wavenumber threshold (FP32 path).  MODE 2: only systems below it.
+template <typename T, typename A, bool CPLX, int MODE, bool CYC>
 __global__ void __launch_bounds__(TPB) k_thomas_z(void* __restrict__ data_, ZSys z, const int* __restrict__ skip,
                                                   int* __restrict__ err)
 {
     if (skip && *skip) return;
-    extern __shared__ double ck[];
     using E = typename Elem<T, CPLX>::type;
     E* data = reinterpret_cast<E*>(data_);
     const long sys = (long)blockIdx.x * TPB + threadIdx.x;
     const int kx = (int)(sys % z.pitch), ky = (int)(sys / z.pitch);
-    const bool valid = (kx < z.mx) && (ky < z.my);
-    if (!valid) return;
+    if (kx >= z.mx || ky >= z.my) return;
 
     Coef co;
     co.am = z.am; co.ap = z.ap;
     co.lx = z.lamx[kx];
     co.ly = z.lamy[ky];
     co.pin = (kx == 0 && ky == 0);
-    const bool fp64 = (sizeof(T) == 8) || ((co.lx + co.ly) * __ldg(z.dzmax2) < z.lowk);
+    if (MODE != 0) {
+        const bool low = (co.lx + co.ly) * __ldg(z.dzmax2) < z.lowk;
+        if ((MODE == 1) == low) return;
+    }
     double zsum = 0.0;
     bool bad = false;
-    if (z.cyclic) {
-        if (fp64) thomas_poisson_cyc<T, double, CPLX>(data, sys, z.plane, z.nz, co, z.scale, ck + threadIdx.x, zsum, bad);
-        else      thomas_poisson_cyc<T, float, CPLX>(data, sys, z.plane, z.nz, co, z.scale, ck + threadIdx.x, zsum, bad);
-    } else {
-        if (fp64) thomas_poisson<T, double, CPLX>(data, sys, z.plane, z.nz, co, z.scale, ck + threadIdx.x, zsum, bad);
-        else      thomas_poisson<T, float, CPLX>(data, sys, z.plane, z.nz, co, z.scale, ck + threadIdx.x, zsum, bad);
-    }
+    double* ck = z.ckpt + sys;
+    if (CYC) thomas_poisson_cyc<T, A, CPLX>(data, sys, z.plane, z.nz, co, z.scale, ck, zsum, bad);
+    else     thomas_poisson<T, A, CPLX>(data, sys, z.plane, z.nz, co, z.scale, ck, zsum, bad);
     if (co.pin && z.dc_shift) *z.dc_shift = zsum / (double)z.nz;
     if (bad && err) atomicOr(err, 1);
 }
 
+long tdma_z_ckpt_doubles(int nz, long plane, int cyclic)
+{
+    const int m = cyclic ? nz - 1 : nz;
+    const int ch = Exact::CH < Fast::CH ? Exact::CH : Fast::CH;   // the finer chunking of the two paths
+    const long nch = (m + ch - 1) / ch;
+    return nch * (cyclic ? 4 : 3) * plane;
+}
+
+namespace {
+template <bool CPLX, bool CYC>
+void launch_z(double*, const ZSys& z, void* data, const int* skip, int* err, cudaStream_t st)
+{
+    dim3 grid((unsigned)((z.plane + TPB - 1) / TPB));  // pitch * my systems incl. padding columns
+    k_thomas_z<double, Exact, CPLX, 0, CYC><<<grid, TPB, 0, st>>>(data, z, skip, err);
+}
+template <bool CPLX, bool CYC>
+void launch_z(float*, const ZSys& z, void* data, const int* skip, int* err, cudaStream_t st)
+{
+    dim3 grid((unsigned)((z.plane + TPB - 1) / TPB));
+    k_thomas_z<float, Fast, CPLX, 1, CYC><<<grid, TPB, 0, st>>>(data, z, skip, err);
+    k_thomas_z<float, Exact, CPLX, 2, CYC><<<grid, TPB, 0, st>>>(data, z, skip, err);
+}
+}  // namespace
+
 template <typename T, bool CPLX>
 cudaError_t launch_tdma_z(void* data, const ZSys& z, const int* skip_flag, int* err_flag, cudaStream_t st)
 {
-    const int nch = (z.nz + CH - 1) / CH;
-    const size_t smem = (size_t)(z.cyclic ? 4 : 3) * nch * TPB * sizeof(double);
-    if (smem > 200 * 1024) return cudaErrorInvalidConfiguration;
-    const long nsys = z.plane;  // pitch * my systems incl. padding columns
-    dim3 grid((unsigned)((nsys + TPB - 1) / TPB));
-    auto kern = k_thomas_z<T, CPLX>;
-    if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-    }
-    kern<<<grid, TPB, smem, st>>>(data, z, skip_flag, err_flag);
+    if (z.cyclic) launch_z<CPLX, true>((T*)nullptr, z, data, skip_flag, err_flag, st);
+    else          launch_z<CPLX, false>((T*)nullptr, z, data, skip_flag, err_flag, st);
     return cudaGetLastError();
 }
 
@@ -414,7 +456,7 @@ __global__ void __launch_bounds__(TPB) k_thomas_arr(const double* __restrict__ a
         ld_chunk(A, z0, n, av, bv, cv, dv);
 #pragma unroll
         for (int r = 0; r < CH; ++r)
-            if (z0 + r < n) fwd_row<double, false>(z0 + r == 0, av[r], bv[r], cv[r], dv[r], 0.0, cp, dp, dum);
+            if (z0 + r < n) fwd_row<Exact, false>(z0 + r == 0, av[r], bv[r], cv[r], dv[r], 0.0, cp, dp, dum);
         my[(2 * ch) * TPB] = cp;
         my[(2 * ch + 1) * TPB] = dp;
     }
@@ -427,7 +469,7 @@ __global__ void __launch_bounds__(TPB) k_thomas_arr(const double* __restrict__ a
         double c_[CH], d_[CH];
 #pragma unroll
         for (int r = 0; r < CH; ++r) {
-            if (z0 + r < n) fwd_row<double, false>(z0 + r == 0, av[r], bv[r], cv[r], dv[r], 0.0, pc, pd, dum);
+            if (z0 + r < n) fwd_row<Exact, false>(z0 + r == 0, av[r], bv[r], cv[r], dv[r], 0.0, pc, pd, dum);
             c_[r] = pc; d_[r] = pd;
         }
 #pragma unroll
@@ -472,7 +514,7 @@ __global__ void __launch_bounds__(TPB) k_thomas_cycl(const double* __restrict__ 
         ld_chunk(A, z0, m, av, bv, cv, dv);
 #pragma unroll
         for (int r = 0; r < CH; ++r)
-            if (z0 + r < m) fwd_row<double, true>(z0 + r == 0, av[r], bv[r], cv[r], dv[r], e_in(z0 + r), cp, dp, ep);
+            if (z0 + r < m) fwd_row<Exact, true>(z0 + r == 0, av[r], bv[r], cv[r], dv[r], e_in(z0 + r), cp, dp, ep);
         my[(3 * ch) * TPB] = cp;
         my[(3 * ch + 1) * TPB] = dp;
         my[(3 * ch + 2) * TPB] = ep;
@@ -497,7 +539,7 @@ __global__ void __launch_bounds__(TPB) k_thomas_cycl(const double* __restrict__ 
             double c_[CH], d_[CH], e_[CH];
 #pragma unroll
             for (int r = 0; r < CH; ++r) {
-                if (z0 + r < m) fwd_row<double, true>(z0 + r == 0, av[r], bv[r], cv[r], dv[r], e_in(z0 + r), pc, pd, pe);
+                if (z0 + r < m) fwd_row<Exact, true>(z0 + r == 0, av[r], bv[r], cv[r], dv[r], e_in(z0 + r), pc, pd, pe);
                 c_[r] = pc; d_[r] = pd; e_[r] = pe;
             }
 #pragma unroll

@@ -1,0 +1,327 @@
+// ppf_x.cu -- x-direction transform kernels of libppf (sm_100a).
+//
+// One CTA transforms W consecutive x-lines (fixed y, z) in shared memory
+// (ppf_fft.cuh): a real FFT through a half-length complex FFT and a split,
+// or a DCT-II with Makhoul's reordering folded into the tile load and the
+// post-twiddle folded into the store.  The reference runs each of these as
+// a cuFFT call bracketed by separate reorder, twiddle, copy and scale
+// passes (01_Fortran/src/fft_3d_poisson.f90:378-419, 561-616, 915-1033);
+// here each is one read and one write of the field.  SH selects the
+// compile-time engine of a common length or the run-time engine.
+#include "ppf_xy_common.cuh"
+
+namespace ppf {
+
+constexpr int ct_log2(int w) { return w <= 1 ? 0 : 1 + ct_log2(w / 2); }
+
+// --------------------------------------------------------------------------
+// x forward: real lines (FP64 input, optionally f - L u) -> half spectrum
+// (R2C, complex rows of nx/2+1) or DCT-II (real rows of nx).
+// --------------------------------------------------------------------------
+template <typename T, bool DCT, bool RESID, typename SH>
+__global__ void __launch_bounds__(512) k_xfwd(const double* __restrict__ f, ResidIn rs, Geom g,
+                                               void* __restrict__ out_, long out_pitch, FftSched sch, int Wrt,
+                                               int lgWrt, const cx<T>* __restrict__ tw_half,
+                                               const cx<T>* __restrict__ tw_n, const cx<T>* __restrict__ tw_dct,
+                                               const int* __restrict__ skip)
+{
+    if (skip && *skip) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<T>* s = reinterpret_cast<cx<T>*>(smem_raw);
+    constexpr bool CT = SH::CT;
+    const int W = CT ? SH::W : Wrt;
+    const int lgW = CT ? ct_log2(SH::W) : lgWrt;
+    const int NTH = CT ? SH::NT : (int)blockDim.x;
+    const int nc = CT ? SH::N : (g.nx >> 1);
+    const int nx = 2 * nc;
+    const long nlines = (long)g.ny * g.nz;
+    const long line0 = (long)blockIdx.x * W;
+    const int E = nc << lgW;
+
+    for (int e = threadIdx.x; e < E; e += NTH) {
+        const int l = e / nc, n = e - l * nc;
+        const long line = line0 + l;
+        cx<T> z = mk<T>((T)0, (T)0);
+        if (line < nlines) {
+            const double* fl = f + line * nx;
+            double a = fl[2 * n], b = fl[2 * n + 1];
+            if (RESID) {
+                const int j = (int)(line % g.ny), k = (int)(line / g.ny);
+                a -= lap_at(rs, g, 2 * n, j, k);
+                b -= lap_at(rs, g, 2 * n + 1, j, k);
+            }
+            z = mk<T>((T)a, (T)b);
+        }
+        s[sidx<T>(n, l, W)] = z;
+    }
+    __syncthreads();
+
+    if (DCT) {
+        // Makhoul order v = [x0, x2, .., x_{n-2}, x_{n-1}, .., x3, x1]
+        // (cuda_Poisson_DCT_f_pre, fft_3d_poisson.f90:915-935), packed as
+        // complex pairs (v_{2m}, v_{2m+1}) for the half-length FFT.
+        constexpr int EPT = CT ? (SH::N * SH::W + SH::NT - 1) / SH::NT : 8;
+        cx<T> tmp[EPT];
+#pragma unroll
+        for (int i = 0; i < EPT; ++i) {
+            const int e = threadIdx.x + i * NTH;
+            if (e < E) {
+                const int l = e / nc, m = e - l * nc;
+                const int q0 = 2 * m, q1 = 2 * m + 1;
+                const T v0 = (q0 < nc) ? s[sidx<T>(q0, l, W)].x : s[sidx<T>(nx - 1 - q0, l, W)].y;
+                const T v1 = (q1 < nc) ? s[sidx<T>(q1, l, W)].x : s[sidx<T>(nx - 1 - q1, l, W)].y;
+                tmp[i] = mk<T>(v0, v1);
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < EPT; ++i) {
+            const int e = threadIdx.x + i * NTH;
+            if (e < E) {
+                const int l = e / nc, m = e - l * nc;
+                s[sidx<T>(m, l, W)] = tmp[i];
+            }
+        }
+        __syncthreads();
+    }
+
+    tile_fft<T, false, SH>(s, sch, W, lgW, tw_half);
+
+    if (!DCT) {
+        cx<T>* out = reinterpret_cast<cx<T>*>(out_);
+        const int Eo = (nc + 1) * W;
+        for (int e = threadIdx.x; e < Eo; e += NTH) {
+            const int l = e / (nc + 1), k = e - l * (nc + 1);
+            const long line = line0 + l;
+            if (line >= nlines) continue;
+            const cx<T> zk = s[sidx<T>(k == nc ? 0 : k, l, W)];
+            const cx<T> zc = conj(s[sidx<T>(k == 0 ? 0 : nc - k, l, W)]);
+            const cx<T> Ev = (zk + zc) * (T)0.5;
+            const cx<T> D = zk - zc;
+            const cx<T> O = mk<T>(D.y * (T)0.5, -D.x * (T)0.5);
+            out[line * out_pitch + k] = Ev + cmul(ldg(tw_n + k), O);
+        }
+    } else {
+        // X_k = 2 Re(e^{-i pi k/(2n)} V_k), V_{n-k} = conj(V_k)
+        // (cuda_Poisson_DCT_f_post, fft_3d_poisson.f90:937-969)
+        T* out = reinterpret_cast<T*>(out_);
+        const int Eo = nx * W;
+        for (int e = threadIdx.x; e < Eo; e += NTH) {
+            const int l = e / nx, k = e - l * nx;
+            const long line = line0 + l;
+            if (line >= nlines) continue;
+            const int kap = (k <= nc) ? k : nx - k;
+            const cx<T> zk = s[sidx<T>(kap == nc ? 0 : kap, l, W)];
+            const cx<T> zc = conj(s[sidx<T>(kap == 0 ? 0 : nc - kap, l, W)]);
+            const cx<T> Ev = (zk + zc) * (T)0.5;
+            const cx<T> D = zk - zc;
+            const cx<T> O = mk<T>(D.y * (T)0.5, -D.x * (T)0.5);
+            cx<T> V = Ev + cmul(ldg(tw_n + kap), O);
+            if (k > nc) V = conj(V);
+            const cx<T> w = ldg(tw_dct + k);
+            out[line * out_pitch + k] = (T)2 * (w.x * V.x - w.y * V.y);
+        }
+    }
+}
+
+// --------------------------------------------------------------------------
+// x inverse: half spectrum (C2R) or DCT coefficients (inverse DCT) ->
+// interior of the ghosted FP64 output.  ACC: u <- (u - mean_prev) + du.
+// partials (optional): per-block [sum du^2, sum u^2, sum u].
+// --------------------------------------------------------------------------
+template <typename T, bool DCT, bool ACC, typename SH>
+__global__ void __launch_bounds__(512) k_xinv(const void* __restrict__ in_, long in_pitch, double* __restrict__ P,
+                                               Geom g, double* __restrict__ partials,
+                                               const double* __restrict__ mean_prev, FftSched sch, int Wrt,
+                                               int lgWrt, const cx<T>* __restrict__ tw_half,
+                                               const cx<T>* __restrict__ tw_n, const cx<T>* __restrict__ tw_dct,
+                                               const int* __restrict__ skip)
+{
+    if (skip && *skip) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<T>* s = reinterpret_cast<cx<T>*>(smem_raw);
+    constexpr bool CT = SH::CT;
+    const int W = CT ? SH::W : Wrt;
+    const int lgW = CT ? ct_log2(SH::W) : lgWrt;
+    const int NTH = CT ? SH::NT : (int)blockDim.x;
+    const int nc = CT ? SH::N : (g.nx >> 1);
+    const int nx = 2 * nc;
+    const long nlines = (long)g.ny * g.nz;
+    const long line0 = (long)blockIdx.x * W;
+    const int E = nc << lgW;
+
+    for (int e = threadIdx.x; e < E; e += NTH) {
+        const int l = e / nc, k = e - l * nc;
+        const long line = line0 + l;
+        cx<T> Z = mk<T>((T)0, (T)0);
+        if (line < nlines) {
+            cx<T> xk, xc;
+            if (!DCT) {
+                const cx<T>* row = reinterpret_cast<const cx<T>*>(in_) + line * in_pitch;
+                xk = row[k];
+                xc = conj(row[nc - k]);
+                if (k == 0) { xk.y = (T)0; xc.y = (T)0; }
+            } else {
+                // b_pre: Zs_j = e^{i pi j/(2n)} (X_j - i X_{n-j}), X_n = 0
+                const T* row = reinterpret_cast<const T*>(in_) + line * in_pitch;
+                const int j0 = k, j1 = nc - k;
+                const T a0 = row[j0], b0 = (j0 == 0) ? (T)0 : row[nx - j0];
+                const T a1 = row[j1], b1 = (j1 == 0) ? (T)0 : row[nx - j1];
+                const cx<T> w0 = ldg(tw_dct + j0), w1 = ldg(tw_dct + j1);
+                const T c0 = w0.x, s0 = -w0.y, c1 = w1.x, s1 = -w1.y;
+                xk = mk<T>(c0 * a0 + s0 * b0, s0 * a0 - c0 * b0);
+                xc = mk<T>(c1 * a1 + s1 * b1, -(s1 * a1 - c1 * b1));
+                if (k == 0) { xk.y = (T)0; xc.y = (T)0; }
+            }
+            const cx<T> Ev = xk + xc;
+            const cx<T> D = xk - xc;
+            const cx<T> O = cmul(D, conj(ldg(tw_n + k)));
+            Z = mk<T>(Ev.x - O.y, Ev.y + O.x);
+        }
+        s[sidx<T>(k, l, W)] = Z;
+    }
+    tile_fft<T, true, SH>(s, sch, W, lgW, tw_half);
+
+    double acc_du = 0.0, acc_u = 0.0, acc_s = 0.0;
+    const double mprev = (ACC && mean_prev) ? *mean_prev : 0.0;
+    const int Eo = nx << lgW;
+    for (int e = threadIdx.x; e < Eo; e += NTH) {
+        const int l = e / nx, i = e - l * nx;
+        const long line = line0 + l;
+        if (line >= nlines) continue;
+        int n = i;
+        // inverse Makhoul order (cuda_Poisson_DCT_b_post, :1013-1033)
+        if (DCT) n = (i & 1) ? (nc + ((nx - 1 - i) >> 1)) : (i >> 1);
+        const cx<T> zv = s[sidx<T>(n >> 1, l, W)];
+        const double x = (double)((n & 1) ? zv.y : zv.x);
+        const int j = (int)(line % g.ny), k = (int)(line / g.ny);
+        const long o = (long)(i + 1) + (long)(j + 1) * g.pstride_y + (long)(k + 1) * g.pstride_z;
+        // refinement: u <- u + du - mean(u), the FP64 mean of the previous
+        // iterate (the residual cannot see constants, so the gauge is kept here)
+        const double un = ACC ? (P[o] - mprev) + x : x;
+        P[o] = un;
+        if (partials) {
+            acc_du += x * x;
+            acc_u += un * un;
+            acc_s += un;
+        }
+    }
+    if (partials) {
+        // deterministic per-block partial sums (reduced in a fixed order by the gate)
+        __shared__ double red[3][32];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            acc_du += __shfl_down_sync(0xffffffffu, acc_du, off);
+            acc_u += __shfl_down_sync(0xffffffffu, acc_u, off);
+            acc_s += __shfl_down_sync(0xffffffffu, acc_s, off);
+        }
+        const int w = threadIdx.x >> 5, nw = (NTH + 31) >> 5;
+        if ((threadIdx.x & 31) == 0) { red[0][w] = acc_du; red[1][w] = acc_u; red[2][w] = acc_s; }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double a = 0, b = 0, c = 0;
+            for (int q = 0; q < nw; ++q) { a += red[0][q]; b += red[1][q]; c += red[2][q]; }
+            partials[3 * blockIdx.x + 0] = a;
+            partials[3 * blockIdx.x + 1] = b;
+            partials[3 * blockIdx.x + 2] = c;
+        }
+    }
+}
+
+// --------------------------------------------------------------------------
+// launchers
+// --------------------------------------------------------------------------
+template <typename T>
+cudaError_t launch_xfwd(bool dct, const double* f, const ResidIn* resid, const Geom& g, void* out, long out_pitch,
+                        const FftSched& sch, const cx<T>* tw_half, const cx<T>* tw_n, const cx<T>* tw_dct,
+                        const int* skip_flag, cudaStream_t st)
+{
+    const int nc = g.nx / 2;
+    ResidIn rs{};
+    if (resid) rs = *resid;
+    cudaError_t err = cudaSuccess;
+    with_shape<T>(nc, [&](auto sh) {
+        using SH = decltype(sh);
+        int W, threads;
+        shape_geom<T, SH>(nc, W, threads);
+        if (threads > 512) { err = cudaErrorInvalidConfiguration; return; }
+        const size_t smem = (size_t)nc * W * sizeof(cx<T>);
+        dim3 grid((unsigned)(((long)g.ny * g.nz + W - 1) / W));
+        auto go = [&](auto kern) {
+            err = set_smem(kern, smem);
+            if (err != cudaSuccess) return;
+            kern<<<grid, threads, smem, st>>>(f, rs, g, out, out_pitch, sch, W, ilog2i(W), tw_half, tw_n, tw_dct,
+                                              skip_flag);
+            err = cudaGetLastError();
+        };
+        if (dct) {
+            if (resid) go(k_xfwd<T, true, true, SH>);
+            else go(k_xfwd<T, true, false, SH>);
+        } else {
+            if (resid) go(k_xfwd<T, false, true, SH>);
+            else go(k_xfwd<T, false, false, SH>);
+        }
+    });
+    return err;
+}
+
+template <typename T>
+cudaError_t launch_xinv(bool dct, const void* in, long in_pitch, double* P, const Geom& g, bool accumulate,
+                        double* partials, const double* mean_prev, const FftSched& sch, const cx<T>* tw_half,
+                        const cx<T>* tw_n, const cx<T>* tw_dct, const int* skip_flag, cudaStream_t st)
+{
+    const int nc = g.nx / 2;
+    cudaError_t err = cudaSuccess;
+    with_shape<T>(nc, [&](auto sh) {
+        using SH = decltype(sh);
+        int W, threads;
+        shape_geom<T, SH>(nc, W, threads);
+        if (threads > 512) { err = cudaErrorInvalidConfiguration; return; }
+        const size_t smem = (size_t)nc * W * sizeof(cx<T>);
+        dim3 grid((unsigned)(((long)g.ny * g.nz + W - 1) / W));
+        auto go = [&](auto kern) {
+            err = set_smem(kern, smem);
+            if (err != cudaSuccess) return;
+            kern<<<grid, threads, smem, st>>>(in, in_pitch, P, g, partials, mean_prev, sch, W, ilog2i(W), tw_half,
+                                              tw_n, tw_dct, skip_flag);
+            err = cudaGetLastError();
+        };
+        if (dct) {
+            if (accumulate) go(k_xinv<T, true, true, SH>);
+            else go(k_xinv<T, true, false, SH>);
+        } else {
+            if (accumulate) go(k_xinv<T, false, true, SH>);
+            else go(k_xinv<T, false, false, SH>);
+        }
+    });
+    return err;
+}
+
+template <typename T>
+long xinv_blocks(const Geom& g)
+{
+    long blocks = 0;
+    with_shape<T>(g.nx / 2, [&](auto sh) {
+        using SH = decltype(sh);
+        int W, threads;
+        shape_geom<T, SH>(g.nx / 2, W, threads);
+        blocks = ((long)g.ny * g.nz + W - 1) / W;
+    });
+    return blocks;
+}
+
+template long xinv_blocks<double>(const Geom&);
+template long xinv_blocks<float>(const Geom&);
+
+#define PPF_INST(T)                                                                                        \
+    template cudaError_t launch_xfwd<T>(bool, const double*, const ResidIn*, const Geom&, void*, long,     \
+                                        const FftSched&, const cx<T>*, const cx<T>*, const cx<T>*,         \
+                                        const int*, cudaStream_t);                                         \
+    template cudaError_t launch_xinv<T>(bool, const void*, long, double*, const Geom&, bool, double*,      \
+                                        const double*, const FftSched&, const cx<T>*, const cx<T>*,        \
+                                        const cx<T>*, const int*, cudaStream_t);
+PPF_INST(double)
+PPF_INST(float)
+#undef PPF_INST
+
+}  // namespace ppf

@@ -1,0 +1,122 @@
+// ppf_xy_common.cuh -- shared pieces of the x and y transform kernels.
+#pragma once
+#include "ppf_fft.cuh"
+#include "ppf_kernels.cuh"
+
+namespace ppf {
+
+// L_h u at cell (i, j, k): 3-point x and y second differences (periodic
+// wrap or mirror at a Neumann wall, uniform spacing) plus the finite-volume
+// z stencil am (u_{k-1} - u) + ap (u_{k+1} - u) -- the operator the
+// transforms and the z solve invert.
+__device__ __forceinline__ double lap_at(const ResidIn& r, const Geom& g, int i, int j, int k)
+{
+    const double* P = r.P;
+    const long base = (long)(i + 1) + (long)(j + 1) * g.pstride_y + (long)(k + 1) * g.pstride_z;
+    const double u = P[base];
+    double uxm, uxp, uym, uyp, uzm, uzp;
+    if (g.px) {
+        uxm = P[base + (i == 0 ? (g.nx - 1) : -1)];
+        uxp = P[base + (i == g.nx - 1 ? -(g.nx - 1) : 1)];
+    } else {
+        uxm = (i == 0) ? u : P[base - 1];
+        uxp = (i == g.nx - 1) ? u : P[base + 1];
+    }
+    if (g.py) {
+        uym = P[base + (j == 0 ? (long)(g.ny - 1) * g.pstride_y : -g.pstride_y)];
+        uyp = P[base + (j == g.ny - 1 ? -(long)(g.ny - 1) * g.pstride_y : g.pstride_y)];
+    } else {
+        uym = (j == 0) ? u : P[base - g.pstride_y];
+        uyp = (j == g.ny - 1) ? u : P[base + g.pstride_y];
+    }
+    uzm = (k == 0) ? u : P[base - g.pstride_z];
+    uzp = (k == g.nz - 1) ? u : P[base + g.pstride_z];
+    const double am = r.am[k], ap = r.ap[k];
+    return (uxm - 2.0 * u + uxp) * r.ix2 + (uym - 2.0 * u + uyp) * r.iy2 + am * (uzm - u) + ap * (uzp - u);
+}
+
+inline int ilog2i(int w)
+{
+    int l = 0;
+    while ((1 << l) < w) ++l;
+    return l;
+}
+
+template <typename K>
+cudaError_t set_smem(K kern, size_t bytes)
+{
+    if (bytes <= 48 * 1024) return cudaSuccess;
+    return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+// run-time tile shape: W lines (a 128-byte bank row of elements when it
+// fits) and >= n*W/8 threads, at most 512
+inline int threads_for(int n, int W)
+{
+    int t = (n * W + 7) / 8;
+    t = (t + 31) & ~31;
+    if (t < 64) t = 64;
+    return t;
+}
+template <typename T>
+inline int pick_w(int n, int& threads)
+{
+    int W = SwizzleG<T>::value;
+    while (W > 1 && threads_for(n, W) > 512) W >>= 1;
+    threads = threads_for(n, W);
+    return W;
+}
+
+// Compile-time shapes of the common lengths: W lines, NT threads (16 FP32
+// or 8 FP64 elements per thread), radix sequence.  Other lengths use the
+// run-time engine.
+template <typename T, typename F>
+void with_shape(int n, F&& f)
+{
+    if constexpr (sizeof(T) == 8) {
+        switch (n) {
+            case 32:  f(ShapeCT<32, 64, 256, 8, 4>{}); return;
+            case 64:  f(ShapeCT<64, 32, 256, 8, 8>{}); return;
+            case 128: f(ShapeCT<128, 16, 256, 8, 4, 4>{}); return;
+            case 256: f(ShapeCT<256, 8, 256, 8, 8, 4>{}); return;
+            case 384: f(ShapeCT<384, 8, 384, 8, 4, 4, 3>{}); return;
+            case 512: f(ShapeCT<512, 8, 512, 8, 8, 8>{}); return;
+            case 768: f(ShapeCT<768, 4, 384, 8, 8, 4, 3>{}); return;
+            default: break;
+        }
+    } else {
+        switch (n) {
+            case 32:  f(ShapeCT<32, 128, 256, 8, 4>{}); return;
+            case 64:  f(ShapeCT<64, 64, 256, 8, 8>{}); return;
+            case 128: f(ShapeCT<128, 32, 256, 8, 4, 4>{}); return;
+            case 256: f(ShapeCT<256, 16, 256, 8, 8, 4>{}); return;
+            case 384: f(ShapeCT<384, 16, 384, 8, 4, 4, 3>{}); return;
+            case 512: f(ShapeCT<512, 16, 512, 8, 8, 8>{}); return;
+            case 768: f(ShapeCT<768, 8, 384, 8, 8, 4, 3>{}); return;
+            default: break;
+        }
+    }
+    f(ShapeRT{});
+}
+
+// launch geometry of a shape for FFT length n (run-time shapes: pick_w)
+template <typename T, typename SH>
+inline void shape_geom(int n, int& W, int& threads)
+{
+    if constexpr (SH::CT) {
+        W = SH::W;
+        threads = SH::NT;
+    } else {
+        W = pick_w<T>(n, threads);
+    }
+}
+
+// FFT of the tile with the shape's engine
+template <typename T, bool INV, typename SH>
+__device__ __forceinline__ void tile_fft(cx<T>* s, const FftSched& sch, int W, int lgW, const cx<T>* __restrict__ tw)
+{
+    if constexpr (SH::CT) SH::template fft<T, INV>(s, tw);
+    else fft_tile<T, INV>(s, sch, W, lgW, tw);
+}
+
+}  // namespace ppf
