@@ -73,6 +73,25 @@ PPF_API int ppf_solve(ppf_plan *plan, const double *f_d, double *p_d,
               const double *dmx1_d, const double *dmx2_d,
               const double *dmx3_d, const double *dx3_d, void *stream);
 
+/* Transpose of the solve map f -> u (interior cells) and, optionally, the
+ * gradient with respect to the z metric arrays.  No reference counterpart:
+ * the reference solve is not differentiable.
+ *   g_d:   dJ/du, PRHS layout (n1m, n2m, n3m), FP64 device.
+ *   df_d:  output dJ/df = M^T g, PRHS layout (may alias g_d).
+ *   u_d:   the forward solution (ghosted P layout, as written by ppf_solve
+ *          with the same metrics); needed only for the metric gradient.
+ *   ddx3_d, ddmx3_d: output dJ/d dx3 and dJ/d dmx3 (n3m+2 doubles, Fortran
+ *          indices 0..n3m+1, entries the solve does not read are 0), or NULL.
+ * J is taken on the interior cells (ghost cells carry no cotangent).  The
+ * adjoint runs one solve with the plan's precision (mixed refinement
+ * included) on diag(1/dx3) g, spectral intermediates are recomputed, not
+ * stored.  The first call on a plan allocates one ghosted FP64 field of
+ * work memory (not capturable); later calls are asynchronous on `stream`. */
+PPF_API int ppf_solve_adjoint(ppf_plan *plan, const double *g_d, double *df_d, const double *u_d,
+              double *ddx3_d, double *ddmx3_d,
+              const double *dmx1_d, const double *dmx2_d,
+              const double *dmx3_d, const double *dx3_d, void *stream);
+
 /* Same as ppf_solve with host arrays: copies in, solves, copies out and
  * synchronises `stream` before returning (the C++ driver's calling model,
  * 00_C/examples/modules.hpp:223-232). */

@@ -134,3 +134,80 @@ def residual(f, P, L1, L2, pbc, dmx3, dx3) -> np.ndarray:
                        _ptr(np.ascontiguousarray(f)), _ptr(np.ascontiguousarray(P)),
                        _ptr(np.ascontiguousarray(dmx3)), _ptr(np.ascontiguousarray(dx3)), _ptr(r))
     return r
+
+
+def zcoef(dmx3, dx3, n3m):
+    """am_k = 1/dx3_k/dmx3_k, ap_k = 1/dx3_k/dmx3_{k+1} with the wall entries
+    zeroed (fft_3d_poisson.f90:1143-1144); index k = 0..n3m-1 is cell k+1."""
+    k = np.arange(1, n3m + 1)
+    am = 1.0 / dx3[k] / dmx3[k]
+    ap = 1.0 / dx3[k] / dmx3[k + 1]
+    am[0] = 0.0
+    ap[-1] = 0.0
+    return am, ap
+
+
+def _zero_mode_matrix(am, ap):
+    """Dense z operator of the (kx, ky) = (0, 0) system with its first row
+    replaced by the pin u_1 = 0 (fft_3d_poisson.f90:1240-1249)."""
+    nz = am.size
+    T = np.zeros((nz, nz))
+    for k in range(nz):
+        T[k, k] = -am[k] - ap[k]
+        if k > 0:
+            T[k, k - 1] = am[k]
+        if k < nz - 1:
+            T[k, k + 1] = ap[k]
+    T[0, :] = 0.0
+    T[0, 0] = 1.0
+    return T
+
+
+def poisson_adjoint(g, L1, L2, pbc, dmx1, dmx2, dmx3, dx3, u=None):
+    """Transpose of the solve map f -> u (interior cells), and optionally the
+    gradient of <g, u> with respect to the z metric arrays.
+
+    The solve is u = P0 M' f: transforms in x and y, one z system per
+    (kx, ky), inverse transforms, arithmetic-mean removal P0.  The x and y
+    operators are symmetric; the z operator is T = V^-1 S with V = diag(dx3)
+    and S symmetric, so T^-T = V T^-1 V^-1 for every system except the
+    pinned zero mode.  Hence M^T g = V M (V^-1 g) + c(z), where c is a
+    per-level constant that swaps the zero mode of V M V^-1 for the exact
+    transposed pinned system (dense solves here).
+
+    With u = M f given (ghosted, as returned by poisson_solve), returns also
+    d<g,u>/d dx3 and d<g,u>/d dmx3 (arrays of n3m+2, Fortran indices 0..n3m+1):
+    dJ/dtheta = -<M^T g, (dL/dtheta) u> with the pinned row excluded.
+    """
+    g = np.ascontiguousarray(g, dtype=np.float64)
+    n3m, n2m, n1m = g.shape
+    nxy = float(n1m * n2m)
+    d3 = np.asarray(dx3, dtype=np.float64)[1:n3m + 1]
+    W = poisson_solve(g / d3[:, None, None], L1, L2, pbc, dmx1, dmx2, dmx3, dx3)[1:-1, 1:-1, 1:-1]
+    am, ap = zcoef(np.asarray(dmx3, dtype=np.float64), np.asarray(dx3, dtype=np.float64), n3m)
+    T = _zero_mode_matrix(am, ap)
+    cs_g = g.sum(axis=(1, 2))
+    rhs = cs_g / d3
+    rhs[0] = 0.0
+    cp = np.linalg.solve(T, rhs) / nxy
+    B = d3 * (cp - cp.mean())
+    cA = np.linalg.solve(T.T, cs_g - cs_g.sum() / n3m) / nxy
+    df = d3[:, None, None] * W + (cA - B)[:, None, None]
+    if u is None:
+        return df
+    ui = np.asarray(u)[1:-1, 1:-1, 1:-1]
+    Sm = np.zeros(n3m)
+    Sp = np.zeros(n3m)
+    Sm[1:] = (df[1:] * (ui[:-1] - ui[1:])).sum(axis=(1, 2))
+    Sp[:-1] = (df[:-1] * (ui[1:] - ui[:-1])).sum(axis=(1, 2))
+    dam, dap = -Sm, -Sp
+    dap[0] += df[0].sum() * (ui[1].sum() - ui[0].sum()) / nxy
+    dam[0] = 0.0
+    dap[-1] = 0.0
+    dmx3 = np.asarray(dmx3, dtype=np.float64)
+    ddx3 = np.zeros(n3m + 2)
+    ddmx3 = np.zeros(n3m + 2)
+    ddx3[1:n3m + 1] = -(dam * am + dap * ap) / d3
+    ddmx3[1:n3m + 1] += -dam * am / dmx3[1:n3m + 1]
+    ddmx3[2:n3m + 2] += -dap * ap / dmx3[2:n3m + 2]
+    return df, ddx3, ddmx3

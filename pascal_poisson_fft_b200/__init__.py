@@ -46,7 +46,7 @@ EXPORTED_SYMBOLS = (
     "ppf_plan_workspace_bytes", "ppf_tdma_many", "ppf_tdma_cycl_many", "ppf_last_error", "ppf_version",
     "ppf_fft_poisson_plan_cuda_create", "ppf_cuda_poisson_fft_initial", "ppf_cuda_poisson_fft_1d",
     "ppf_cuda_poisson_fft_clean", "ppf_cuda_poisson_fft_set_precision", "ppf_stage_timing",
-    "ppf_stage_times", "ppf_solve_noalloc",
+    "ppf_stage_times", "ppf_solve_noalloc", "ppf_solve_adjoint",
 )
 STAGES = ("z-coefficients", "x-forward", "y-forward", "tdma-z", "y-inverse", "x-inverse",
           "refine-gate", "ghost-cells")
@@ -96,6 +96,7 @@ def lib() -> ctypes.CDLL:
     L.ppf_stage_timing.argtypes = [_vp, ctypes.c_int]
     L.ppf_solve_noalloc.argtypes = [ctypes.POINTER(_Desc)] + [_vp] * 6 + [_vp]
     L.ppf_stage_times.argtypes = [_vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)]
+    L.ppf_solve_adjoint.argtypes = [_vp] * 10 + [_vp]
     for name in EXPORTED_SYMBOLS:
         if name not in ("ppf_last_error", "ppf_version"):
             getattr(L, name).restype = ctypes.c_int
@@ -200,6 +201,21 @@ class Plan:
                 _dptr(dmx1, "dmx1", n1m + 2), _dptr(dmx2, "dmx2", n2m + 2),
                 _dptr(dmx3, "dmx3", n3m + 2), _dptr(dx3, "dx3", n3m + 2)]
         _check("ppf_solve", lib().ppf_solve(self._h, *args, _stream_ptr(stream)))
+
+    def solve_adjoint(self, g, df, dmx1, dmx2, dmx3, dx3, u=None, ddx3=None, ddmx3=None,
+                      stream=None) -> None:
+        """Asynchronous transpose solve: df = M^T g (both (n3m,n2m,n1m)); with
+        the forward solution u (ghosted) also d<g,u>/d dx3 and d<g,u>/d dmx3
+        into ddx3, ddmx3 (n3m+2 each)."""
+        n3m, n2m, n1m = self.shape
+        cells = n1m * n2m * n3m
+        up = _dptr(u, "u", (n1m + 2) * (n2m + 2) * (n3m + 2)) if u is not None else None
+        gx = _dptr(ddx3, "ddx3", n3m + 2) if ddx3 is not None else None
+        gm = _dptr(ddmx3, "ddmx3", n3m + 2) if ddmx3 is not None else None
+        args = [_dptr(g, "g", cells), _dptr(df, "df", cells), up, gx, gm,
+                _dptr(dmx1, "dmx1", n1m + 2), _dptr(dmx2, "dmx2", n2m + 2),
+                _dptr(dmx3, "dmx3", n3m + 2), _dptr(dx3, "dx3", n3m + 2)]
+        _check("ppf_solve_adjoint", lib().ppf_solve_adjoint(self._h, *args, _stream_ptr(stream)))
 
     def solve_host(self, f: np.ndarray, dmx1, dmx2, dmx3, dx3, P: np.ndarray | None = None,
                    stream=None) -> np.ndarray:

@@ -116,6 +116,11 @@ struct ppf_plan {
     double* f_dev = nullptr;
     double* p_dev = nullptr;
     double* m_dev = nullptr;
+    // work memory of ppf_solve_adjoint (allocated on first use)
+    double* adj_W = nullptr;       // ghosted solution of the scaled right-hand side
+    double* adj_red = nullptr;     // plane partial sums (5 * nz * nchunk), correction (nz), scratch (4 * nz)
+    long adj_chunk = 0;
+    int adj_nchunk = 0;
     // per-stage timing (ppf_stage_timing)
     bool timing = false;
     std::vector<std::pair<int, cudaEvent_t>> marks;   // stage id (-1 = start), event
@@ -168,7 +173,8 @@ void free_plan(ppf_plan* p)
     if (!p) return;
     drop_marks(p);
     void* ptrs[] = { p->A, p->B, p->lamx, p->lamy, p->am, p->ap, p->scal, p->flags, p->tw,
-                     p->f_dev, p->p_dev, p->m_dev, p->partials, p->ckpt };
+                     p->f_dev, p->p_dev, p->m_dev, p->partials, p->ckpt,
+                     p->adj_W, p->adj_red };
     for (void* q : ptrs)
         if (q) cudaFree(q);
     delete p;
@@ -377,6 +383,53 @@ int solve_impl(ppf_plan* p, const double* f, double* P, const double* dmx1, cons
     return PPF_OK;
 }
 
+// Transpose of the solve (ppf_adjoint.cu has the derivation): df = M^T g,
+// and with u the z-metric gradient of <g, u>.
+int adjoint_impl(ppf_plan* p, const double* g, double* df, const double* u, double* ddx3, double* ddmx3,
+                 const double* dmx1, const double* dmx2, const double* dmx3, const double* dx3, cudaStream_t st)
+{
+    if (!p) return fail(PPF_ERR_INVALID, "null plan");
+    if (!g || !df || !dmx1 || !dmx2 || !dmx3 || !dx3) return fail(PPF_ERR_INVALID, "null array argument");
+    if ((ddx3 || ddmx3) && !u) return fail(PPF_ERR_INVALID, "metric gradients need the forward solution u");
+    int cur = -1;
+    PPF_CK(cudaGetDevice(&cur));
+    if (cur != p->dev) return fail(PPF_ERR_STATE, "plan was created on device %d, current device is %d", p->dev, cur);
+    const Geom& gm = p->g;
+    const int nz = gm.nz;
+    if (!p->adj_W) {
+        p->adj_nchunk = adjoint_chunks((long)gm.nx * gm.ny, &p->adj_chunk);
+        const size_t wb = sizeof(double) * (size_t)(gm.nx + 2) * (gm.ny + 2) * (nz + 2);
+        const size_t rb = sizeof(double) * ((size_t)5 * nz * p->adj_nchunk + 5 * (size_t)nz);
+        if (cudaMalloc(&p->adj_W, wb) != cudaSuccess) {
+            cudaGetLastError();
+            p->adj_W = nullptr;
+            return fail(PPF_ERR_NOMEM, "cannot allocate %.1f MB of adjoint work memory", wb / 1048576.0);
+        }
+        PPF_CK(cudaMalloc(&p->adj_red, rb));
+    }
+    const int nch = p->adj_nchunk;
+    double* colpart = p->adj_red;
+    double* mpart = colpart + (size_t)nz * nch;
+    double* corr = mpart + (size_t)4 * nz * nch;
+    double* wk = corr + nz;
+    // h = (g - plane means) / dx3 into df (aliasing g is allowed), plane sums of g
+    cudaError_t e = launch_adj_rhs(g, df, dx3, gm, p->adj_chunk, nch, colpart, st);
+    if (e != cudaSuccess) return cuda_fail(e, "adjoint right-hand side");
+    // W = M h with the plan's precision (refinement included); this also
+    // computes the z coefficients am, ap used below
+    int rc = solve_impl(p, df, p->adj_W, dmx1, dmx2, dmx3, dx3, st);
+    if (rc != PPF_OK) return rc;
+    e = launch_adj_corr(colpart, nch, gm, p->am, p->ap, corr, wk, st);
+    if (e != cudaSuccess) return cuda_fail(e, "adjoint zero mode");
+    e = launch_adj_out(p->adj_W, df, dx3, corr, (ddx3 || ddmx3) ? u : nullptr, gm, p->adj_chunk, nch, mpart, st);
+    if (e != cudaSuccess) return cuda_fail(e, "adjoint output");
+    if (ddx3 || ddmx3) {
+        e = launch_adj_metric(mpart, nch, gm, p->am, p->ap, dx3, dmx3, ddx3, ddmx3, wk, st);
+        if (e != cudaSuccess) return cuda_fail(e, "adjoint metric gradient");
+    }
+    return PPF_OK;
+}
+
 // one module-global plan for the reference-shaped API (p_poi, fft_3d_poisson.f90:43-59)
 std::mutex g_mod_mu;
 ppf_desc g_mod_desc{};
@@ -457,6 +510,13 @@ int ppf_solve(ppf_plan* plan, const double* f_d, double* p_d, const double* dmx1
 {
     g_err[0] = 0;
     return solve_impl(plan, f_d, p_d, dmx1_d, dmx2_d, dmx3_d, dx3_d, (cudaStream_t)stream);
+}
+
+int ppf_solve_adjoint(ppf_plan* plan, const double* g_d, double* df_d, const double* u_d, double* ddx3_d,
+                      double* ddmx3_d, const double* dmx1_d, const double* dmx2_d, const double* dmx3_d,
+                      const double* dx3_d, void* stream)
+{
+    return adjoint_impl(plan, g_d, df_d, u_d, ddx3_d, ddmx3_d, dmx1_d, dmx2_d, dmx3_d, dx3_d, (cudaStream_t)stream);
 }
 
 int ppf_solve_host(ppf_plan* plan, const double* f_h, double* p_h, const double* dmx1_h, const double* dmx2_h,

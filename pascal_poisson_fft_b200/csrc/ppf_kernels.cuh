@@ -101,4 +101,17 @@ cudaError_t launch_sweep_gate(const double* partials, long nblocks, double ncell
                               int* skip_flag, int* sweeps_done, double* last_rel, double tol, int initial,
                               cudaStream_t st);
 
+// ---- transpose of the solve and z-metric gradient (ppf_adjoint.cu) ----
+// per-level reductions run over nchunk blocks of `chunk` cells of a plane
+int adjoint_chunks(long plane, long* chunk);
+cudaError_t launch_adj_rhs(const double* g, double* h, const double* dx3, const Geom& gm, long chunk, int nchunk,
+                           double* colpart, cudaStream_t st);
+cudaError_t launch_adj_corr(const double* colpart, int nchunk, const Geom& gm, const double* am, const double* ap,
+                            double* corr, double* wk, cudaStream_t st);
+cudaError_t launch_adj_out(const double* W, double* df, const double* dx3, const double* corr, const double* u,
+                           const Geom& gm, long chunk, int nchunk, double* mpart, cudaStream_t st);
+cudaError_t launch_adj_metric(const double* mpart, int nchunk, const Geom& gm, const double* am, const double* ap,
+                              const double* dx3, const double* dmx3, double* ddx3, double* ddmx3, double* wk,
+                              cudaStream_t st);
+
 }  // namespace ppf

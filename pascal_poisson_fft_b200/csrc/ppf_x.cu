@@ -13,6 +13,7 @@
 namespace ppf {
 
 constexpr int ct_log2(int w) { return w <= 1 ? 0 : 1 + ct_log2(w / 2); }
+constexpr int MAXW = 128;  // widest tile of any shape (FP32, n = 32)
 
 // --------------------------------------------------------------------------
 // x forward: real lines (FP64 input, optionally f - L u) -> half spectrum
@@ -37,6 +38,16 @@ __global__ void __launch_bounds__(512) k_xfwd(const double* __restrict__ f, Resi
     const long nlines = (long)g.ny * g.nz;
     const long line0 = (long)blockIdx.x * W;
     const int E = nc << lgW;
+    // (y, z) of each line of the tile, computed once (no per-element division)
+    __shared__ int line_j[MAXW], line_k[MAXW];
+    if (RESID) {
+        for (int l = threadIdx.x; l < W; l += NTH) {
+            const long line = line0 + l;
+            line_j[l] = (int)(line % g.ny);
+            line_k[l] = (int)(line / g.ny);
+        }
+        __syncthreads();
+    }
 
     for (int e = threadIdx.x; e < E; e += NTH) {
         const int l = e / nc, n = e - l * nc;
@@ -46,7 +57,7 @@ __global__ void __launch_bounds__(512) k_xfwd(const double* __restrict__ f, Resi
             const double* fl = f + line * nx;
             double a = fl[2 * n], b = fl[2 * n + 1];
             if (RESID) {
-                const int j = (int)(line % g.ny), k = (int)(line / g.ny);
+                const int j = line_j[l], k = line_k[l];
                 a -= lap_at(rs, g, 2 * n, j, k);
                 b -= lap_at(rs, g, 2 * n + 1, j, k);
             }
@@ -180,6 +191,14 @@ __global__ void __launch_bounds__(512) k_xinv(const void* __restrict__ in_, long
         }
         s[sidx<T>(k, l, W)] = Z;
     }
+    // ghosted-output offset of each line of the tile (no per-element division)
+    __shared__ long line_base[MAXW];
+    for (int l = threadIdx.x; l < W; l += NTH) {
+        const long line = line0 + l;
+        const long j = line % g.ny, k = line / g.ny;
+        line_base[l] = 1 + (j + 1) * g.pstride_y + (k + 1) * g.pstride_z;
+    }
+    __syncthreads();
     tile_fft<T, true, SH>(s, sch, W, lgW, tw_half);
 
     double acc_du = 0.0, acc_u = 0.0, acc_s = 0.0;
@@ -194,8 +213,7 @@ __global__ void __launch_bounds__(512) k_xinv(const void* __restrict__ in_, long
         if (DCT) n = (i & 1) ? (nc + ((nx - 1 - i) >> 1)) : (i >> 1);
         const cx<T> zv = s[sidx<T>(n >> 1, l, W)];
         const double x = (double)((n & 1) ? zv.y : zv.x);
-        const int j = (int)(line % g.ny), k = (int)(line / g.ny);
-        const long o = (long)(i + 1) + (long)(j + 1) * g.pstride_y + (long)(k + 1) * g.pstride_z;
+        const long o = line_base[l] + i;
         // refinement: u <- u + du - mean(u), the FP64 mean of the previous
         // iterate (the residual cannot see constants, so the gauge is kept here)
         const double un = ACC ? (P[o] - mprev) + x : x;

@@ -151,6 +151,17 @@ def config3_field(p: Problem, seed: int, modes: int = 48, noise: float = 1e-3, d
     return f
 
 
+def config5(seed: int = 5, n1m: int = 256, n2m: int = 256, n3m: int = 128, beta: float = 2.0,
+            modes: int = 48, noise: float = 1e-3):
+    """Differentiation workload: periodic x,y, tanh z (beta); the right-hand
+    side f and the right-hand side f_tgt whose solve is the target u_tgt of
+    J = 1/2 ||u - u_tgt||^2, both seeded random-mode fields (config3_field).
+    Returns (problem with f, f_tgt)."""
+    p = build_metrics(Problem("c5", n1m, n2m, n3m, TWO_PI, TWO_PI, 1.0, (True, True, False), beta))
+    p.f = config3_field(p, seed, modes, noise)
+    return p, config3_field(p, seed + 1000, modes, noise)
+
+
 def manufactured(n: int, pbc=(True, True, False), L: float = 2.0):
     """u = cos(pi x) cos(pi y) cos(pi z) on [0,L]^3 with f = -3 pi^2 u
     (module_solve_poisson.f90:127-209); exact for the continuous problem."""
