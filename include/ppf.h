@@ -92,6 +92,28 @@ PPF_API int ppf_solve_adjoint(ppf_plan *plan, const double *g_d, double *df_d, c
               const double *dmx1_d, const double *dmx2_d,
               const double *dmx3_d, const double *dx3_d, void *stream);
 
+/* Batched solves of independent problems of uneven shape and boundary
+ * conditions.  No reference counterpart (the reference solves one grid per
+ * rank).  ppf_batch_create builds a plan per descriptor, spreads the
+ * problems over `branches` concurrent branches (<= 0: 8) with one work
+ * area per branch, and with PPF_BATCH_AUTOTUNE times the candidate tile
+ * widths and radix orders of every distinct x and y transform on the
+ * device and keeps the fastest.  ppf_batch_solve takes host arrays of
+ * `count` device pointers (layouts as ppf_solve); the first call, and any
+ * call with different pointers, captures all problems into one CUDA graph
+ * (not itself capturable); every call then replays it with one graph launch
+ * on `stream`.  ppf_batch_info(batch, i, info[8]): branch of problem i,
+ * x tile width / run-time engine / radix order, the same for y, and the
+ * number of branches (0 width = default). */
+typedef struct ppf_batch ppf_batch;
+#define PPF_BATCH_AUTOTUNE 1
+PPF_API int ppf_batch_create(const ppf_desc *descs, int count, int flags, int branches, ppf_batch **batch);
+PPF_API int ppf_batch_destroy(ppf_batch *batch);
+PPF_API int ppf_batch_solve(ppf_batch *batch, const double *const *f_d, double *const *p_d,
+              const double *const *dmx1_d, const double *const *dmx2_d,
+              const double *const *dmx3_d, const double *const *dx3_d, void *stream);
+PPF_API int ppf_batch_info(const ppf_batch *batch, int index, int *info);
+
 /* Same as ppf_solve with host arrays: copies in, solves, copies out and
  * synchronises `stream` before returning (the C++ driver's calling model,
  * 00_C/examples/modules.hpp:223-232). */

@@ -30,7 +30,7 @@ from dataclasses import dataclass
 import numpy as np
 
 __all__ = [
-    "PPF_FP64", "PPF_MIXED", "PPF_FP32", "PPFError", "lib", "Plan", "mesh",
+    "PPF_FP64", "PPF_MIXED", "PPF_FP32", "PPF_BATCH_AUTOTUNE", "PPFError", "lib", "Plan", "Batch", "mesh",
     "fft_poisson_plan_cuda_create", "cuda_Poisson_FFT_initial", "cuda_Poisson_FFT_1D",
     "cuda_Poisson_FFT_clean", "PaScaL_TDMA_many_solve_cuda", "PaScaL_TDMA_many_solve_cycle_cuda",
     "tdma_many", "tdma_cycl_many", "EXPORTED_SYMBOLS",
@@ -46,8 +46,10 @@ EXPORTED_SYMBOLS = (
     "ppf_plan_workspace_bytes", "ppf_tdma_many", "ppf_tdma_cycl_many", "ppf_last_error", "ppf_version",
     "ppf_fft_poisson_plan_cuda_create", "ppf_cuda_poisson_fft_initial", "ppf_cuda_poisson_fft_1d",
     "ppf_cuda_poisson_fft_clean", "ppf_cuda_poisson_fft_set_precision", "ppf_stage_timing",
-    "ppf_stage_times", "ppf_solve_noalloc", "ppf_solve_adjoint",
+    "ppf_stage_times", "ppf_solve_noalloc", "ppf_solve_adjoint", "ppf_batch_create", "ppf_batch_destroy",
+    "ppf_batch_solve", "ppf_batch_info",
 )
+PPF_BATCH_AUTOTUNE = 1
 STAGES = ("z-coefficients", "x-forward", "y-forward", "tdma-z", "y-inverse", "x-inverse",
           "refine-gate", "ghost-cells")
 
@@ -97,6 +99,11 @@ def lib() -> ctypes.CDLL:
     L.ppf_solve_noalloc.argtypes = [ctypes.POINTER(_Desc)] + [_vp] * 6 + [_vp]
     L.ppf_stage_times.argtypes = [_vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)]
     L.ppf_solve_adjoint.argtypes = [_vp] * 10 + [_vp]
+    L.ppf_batch_create.argtypes = [ctypes.POINTER(_Desc), ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                   ctypes.POINTER(_vp)]
+    L.ppf_batch_destroy.argtypes = [_vp]
+    L.ppf_batch_solve.argtypes = [_vp] + [ctypes.POINTER(_vp)] * 6 + [_vp]
+    L.ppf_batch_info.argtypes = [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     for name in EXPORTED_SYMBOLS:
         if name not in ("ppf_last_error", "ppf_version"):
             getattr(L, name).restype = ctypes.c_int
@@ -248,6 +255,65 @@ class Plan:
         _check("ppf_last_sweeps", lib().ppf_last_sweeps(self._h, ctypes.byref(s), ctypes.byref(r),
                                                         _stream_ptr(stream)))
         return s.value, r.value
+
+
+class Batch:
+    """Independent problems of uneven shape solved by one graph launch.
+
+    problems: sequence of dicts with keys n1m, n2m, n3m, L1, L2, pbc (3-tuple),
+    and optionally precision, max_sweeps, sweep_tol, lowk_threshold."""
+
+    def __init__(self, problems, autotune=True, branches=0):
+        descs = (_Desc * len(problems))()
+        self.shapes = []
+        for k, q in enumerate(problems):
+            pbc = q.get("pbc", (1, 1, 0))
+            descs[k] = _Desc(q["n1m"], q["n2m"], q["n3m"], float(q["L1"]), float(q["L2"]),
+                             int(bool(pbc[0])), int(bool(pbc[1])), int(bool(pbc[2])),
+                             int(q.get("precision", PPF_FP64)), int(q.get("max_sweeps", -1)),
+                             float(q.get("sweep_tol", 0.0)), float(q.get("lowk_threshold", 0.0)))
+            self.shapes.append((q["n3m"], q["n2m"], q["n1m"]))
+        self._h = _vp()
+        _check("ppf_batch_create", lib().ppf_batch_create(descs, len(problems),
+                                                          PPF_BATCH_AUTOTUNE if autotune else 0,
+                                                          int(branches), ctypes.byref(self._h)))
+
+    def __len__(self):
+        return len(self.shapes)
+
+    def close(self) -> None:
+        if self._h:
+            lib().ppf_batch_destroy(self._h)
+            self._h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def solve(self, fs, Ps, dmx1s, dmx2s, dmx3s, dx3s, stream=None) -> None:
+        """Asynchronous: every problem k solves fs[k] -> Ps[k] (torch CUDA float64)."""
+        n = len(self.shapes)
+        arrs = []
+        for name, ts, extra in (("f", fs, 0), ("P", Ps, 2), ("dmx1", dmx1s, -1), ("dmx2", dmx2s, -2),
+                                ("dmx3", dmx3s, -3), ("dx3", dx3s, -3)):
+            if len(ts) != n:
+                raise ValueError(f"{name}: {len(ts)} arrays for {n} problems")
+            a = (_vp * n)()
+            for k, t in enumerate(ts):
+                n3m, n2m, n1m = self.shapes[k]
+                numel = {0: n1m * n2m * n3m, 2: (n1m + 2) * (n2m + 2) * (n3m + 2),
+                         -1: n1m + 2, -2: n2m + 2, -3: n3m + 2}[extra]
+                a[k] = _dptr(t, f"{name}[{k}]", numel)
+            arrs.append(a)
+        _check("ppf_batch_solve", lib().ppf_batch_solve(self._h, *arrs, _stream_ptr(stream)))
+
+    def info(self, k: int) -> dict:
+        v = (ctypes.c_int * 8)()
+        _check("ppf_batch_info", lib().ppf_batch_info(self._h, int(k), v))
+        return dict(branch=v[0], x_width=v[1], x_runtime=v[2], x_order=v[3],
+                    y_width=v[4], y_runtime=v[5], y_order=v[6], branches=v[7])
 
 
 # ---- reference-shaped module API ------------------------------------------

@@ -1,6 +1,7 @@
 // ppf_api.cu -- plans, solve orchestration and the C ABI of libppf.
 #include "../../include/ppf.h"
 #include "ppf_kernels.cuh"
+#include "ppf_xy_common.cuh"
 
 #include <cuda_runtime.h>
 
@@ -8,7 +9,11 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <algorithm>
+#include <array>
+#include <map>
 #include <mutex>
+#include <tuple>
 #include <new>
 #include <vector>
 
@@ -51,15 +56,17 @@ void cexp_tab(int count, long double num, long double den, std::vector<double>& 
     }
 }
 
-bool factor(int n, FftSched& s)
+// Radix schedule of a length-n transform.  order 0: radix 8 first, then 4,
+// 2, 3, 5 (fewest passes); 1: no radix 8; 2: radices 3 and 5 first.
+bool factor(int n, FftSched& s, int order_id = 0)
 {
+    static const int orders[3][5] = { { 8, 4, 2, 3, 5 }, { 4, 2, 3, 5, 0 }, { 3, 5, 8, 4, 2 } };
+    s = FftSched{};
     s.n = n;
-    s.npass = 0;
+    if (n < 1 || order_id < 0 || order_id > 2) return false;
     int m = n;
-    if (n < 1) return false;
-    const int order[5] = { 8, 4, 2, 3, 5 };
-    for (int r : order) {
-        while (m % r == 0 && m > 1) {
+    for (int r : orders[order_id]) {
+        while (r > 0 && m % r == 0 && m > 1) {
             if (s.npass >= 12) return false;
             s.radix[s.npass++] = r;
             m /= r;
@@ -108,6 +115,8 @@ struct ppf_plan {
     double* partials = nullptr;  // per-block sums of the x-inverse pass (mixed precision)
     long xinv_nblk = 0;
     double* ckpt = nullptr;      // Thomas checkpoints of the z solve
+    long ckpt_doubles = 0;
+    bool own_work = true;        // A, B, ckpt, partials belong to the plan (not to a batch)
     void* tw = nullptr;        // twiddle tables (type T)
     size_t tw_off[5] = {};     // element offsets: x half, x n, x dct, y n, y dct
     FftSched sx{}, sy{};
@@ -172,11 +181,15 @@ void free_plan(ppf_plan* p)
 {
     if (!p) return;
     drop_marks(p);
-    void* ptrs[] = { p->A, p->B, p->lamx, p->lamy, p->am, p->ap, p->scal, p->flags, p->tw,
-                     p->f_dev, p->p_dev, p->m_dev, p->partials, p->ckpt,
-                     p->adj_W, p->adj_red };
+    void* ptrs[] = { p->lamx, p->lamy, p->am, p->ap, p->scal, p->flags, p->tw,
+                     p->f_dev, p->p_dev, p->m_dev, p->adj_W, p->adj_red };
     for (void* q : ptrs)
         if (q) cudaFree(q);
+    if (p->own_work) {
+        void* work[] = { p->A, p->B, p->partials, p->ckpt };
+        for (void* q : work)
+            if (q) cudaFree(q);
+    }
     delete p;
 }
 
@@ -264,11 +277,6 @@ int plan_init(ppf_plan* p, const ppf_desc* d)
         if (!p->xdct && j + 1 > ny / 2 + 1) jm = ny - j;   // periodic-periodic fold (:339-346)
         ly[j] = wn_fft(jm, ny, hy);
     }
-    if (cudaMalloc(&p->A, p->a_bytes) != cudaSuccess || cudaMalloc(&p->B, p->b_bytes) != cudaSuccess) {
-        cudaGetLastError();
-        return fail(PPF_ERR_NOMEM, "cannot allocate %.1f MB of spectral work memory",
-                    (p->a_bytes + p->b_bytes) / 1048576.0);
-    }
     PPF_CK(cudaMalloc(&p->lamx, sizeof(double) * p->mx));
     PPF_CK(cudaMalloc(&p->lamy, sizeof(double) * p->my));
     PPF_CK(cudaMalloc(&p->am, sizeof(double) * nz));
@@ -277,15 +285,36 @@ int plan_init(ppf_plan* p, const ppf_desc* d)
     PPF_CK(cudaMalloc(&p->flags, sizeof(int) * 4));
     PPF_CK(cudaMemset(p->scal, 0, sizeof(double) * 8));
     PPF_CK(cudaMemset(p->flags, 0, sizeof(int) * 4));
-    if (p->d.precision == PPF_MIXED) {
-        p->xinv_nblk = xinv_blocks<float>(p->g);
-        PPF_CK(cudaMalloc(&p->partials, sizeof(double) * 3 * p->xinv_nblk));
-    }
-    PPF_CK(cudaMalloc(&p->ckpt, sizeof(double) * tdma_z_ckpt_doubles(nz, p->b_pitch * (long)p->my, p->g.pz)));
+    p->ckpt_doubles = tdma_z_ckpt_doubles(nz, p->b_pitch * (long)p->my, p->g.pz);
     PPF_CK(cudaMemcpy(p->lamx, lx.data(), sizeof(double) * p->mx, cudaMemcpyHostToDevice));
     PPF_CK(cudaMemcpy(p->lamy, ly.data(), sizeof(double) * p->my, cudaMemcpyHostToDevice));
     int rc = (p->elem == 8) ? upload_twiddles<double>(p) : upload_twiddles<float>(p);
     return rc;
+}
+
+// blocks of the x-inverse pass with the plan's current x schedule (mixed
+// precision keeps 3 partial sums per block)
+long partials_doubles(const ppf_plan* p)
+{
+    return (p->d.precision == PPF_MIXED) ? 3 * xinv_blocks<float>(p->g, p->sx) : 0;
+}
+
+// the plan's own work memory: spectral buffers, Thomas checkpoints, partials
+int plan_alloc_work(ppf_plan* p)
+{
+    p->own_work = true;
+    if (cudaMalloc(&p->A, p->a_bytes) != cudaSuccess || cudaMalloc(&p->B, p->b_bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(PPF_ERR_NOMEM, "cannot allocate %.1f MB of spectral work memory",
+                    (p->a_bytes + p->b_bytes) / 1048576.0);
+    }
+    PPF_CK(cudaMalloc(&p->ckpt, sizeof(double) * p->ckpt_doubles));
+    const long np = partials_doubles(p);
+    if (np > 0) {
+        p->xinv_nblk = np / 3;
+        PPF_CK(cudaMalloc(&p->partials, sizeof(double) * np));
+    }
+    return PPF_OK;
 }
 
 template <typename T>
@@ -455,6 +484,7 @@ int ppf_plan_create(const ppf_desc* desc, ppf_plan** plan)
     ppf_plan* p = new (std::nothrow) ppf_plan();
     if (!p) return fail(PPF_ERR_NOMEM, "host allocation failed");
     rc = plan_init(p, desc);
+    if (rc == PPF_OK) rc = plan_alloc_work(p);
     if (rc != PPF_OK) {
         free_plan(p);
         return rc;
@@ -837,3 +867,387 @@ extern "C" int ppf_solve_noalloc(const ppf_desc* desc, const double* f_d, double
     p.ckpt = nullptr;
     return rc;
 }
+
+// ===========================================================================
+// Batched solves of independent problems of uneven shape (ppf_batch_*).
+//
+// Each problem keeps a plan (tables, twiddles, schedules); the problems are
+// spread over a few concurrent branches by estimated cost (longest first,
+// each to the least-loaded branch), and every branch owns one set of work
+// buffers sized for its largest problem, which its problems use in turn.
+// The whole batch -- every problem's launches on its branch, branches
+// forked from and joined to one origin -- is captured once into a CUDA
+// graph and replayed with a single graph launch per ppf_batch_solve.
+// With PPF_BATCH_AUTOTUNE, the tile width and radix order of every
+// distinct x and y transform are picked by timing the candidates on the
+// device before the capture.
+// ===========================================================================
+struct ppf_batch {
+    std::vector<ppf_plan*> plans;
+    std::vector<std::vector<int>> order;     // problems of each branch, in launch order
+    std::vector<std::array<int, 8>> info;    // per problem: branch, x (w, rt, order), y (w, rt, order), 0
+    std::vector<void*> work;                 // owned work buffers
+    std::vector<cudaStream_t> streams;       // [0] capture origin, [1..] branches
+    std::vector<cudaEvent_t> events;         // [0] fork, [1..] joins
+    cudaGraphExec_t exec = nullptr;
+    std::vector<const void*> key;            // pointers the graph was captured with
+    int dev = 0;
+};
+
+namespace {
+
+void free_batch(ppf_batch* b)
+{
+    if (!b) return;
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    for (auto* p : b->plans) free_plan(p);
+    for (void* w : b->work)
+        if (w) cudaFree(w);
+    for (auto s : b->streams)
+        if (s) cudaStreamDestroy(s);
+    for (auto e : b->events)
+        if (e) cudaEventDestroy(e);
+    delete b;
+}
+
+struct TuneKey {
+    int axis, n, kind, elem;
+    bool operator<(const TuneKey& o) const
+    {
+        return std::tie(axis, n, kind, elem) < std::tie(o.axis, o.n, o.kind, o.elem);
+    }
+};
+struct TuneChoice {
+    FftSched s;
+    int order;
+};
+
+// candidate schedules of one transform length: the compile-time shape when
+// one exists, and run-time shapes over radix orders and tile widths
+template <typename T>
+std::vector<TuneChoice> tune_candidates(int n)
+{
+    std::vector<TuneChoice> out;
+    TuneChoice base{};
+    factor(n, base.s, 0);
+    out.push_back(base);  // default (compile-time shape where one exists)
+    int thr = 0;
+    const int w0 = pick_w<T>(n, thr);
+    for (int o = 0; o < 3; ++o) {
+        TuneChoice c{};
+        if (!factor(n, c.s, o)) continue;
+        bool dup = false;
+        for (int q = 0; q < o && !dup; ++q) {
+            FftSched t{};
+            factor(n, t, q);
+            dup = (t.npass == c.s.npass) && std::equal(t.radix, t.radix + t.npass, c.s.radix);
+        }
+        if (dup) continue;
+        for (int w : { w0 / 2, w0, 2 * w0, 4 * w0 }) {
+            if (!width_ok<T>(n, w)) continue;
+            TuneChoice r = c;
+            r.s.rt = 1;
+            r.s.w = w;
+            r.order = o;
+            out.push_back(r);
+        }
+    }
+    return out;
+}
+
+template <typename T>
+int time_axis(ppf_plan* p, int axis, const FftSched& s, const double* f, double* P, cudaStream_t st,
+              cudaEvent_t e0, cudaEvent_t e1, float* ms)
+{
+    const cx<T>* tw = reinterpret_cast<const cx<T>*>(p->tw);
+    const cx<T>* txh = tw + p->tw_off[0];
+    const cx<T>* txn = tw + p->tw_off[1];
+    const cx<T>* txd = tw + p->tw_off[2];
+    const cx<T>* tyn = tw + p->tw_off[3];
+    const cx<T>* tyd = tw + p->tw_off[4];
+    const long a_cp = p->xdct ? p->a_pitch / 2 : p->a_pitch;
+    const long b_cp = (p->xdct && p->ydct) ? p->b_pitch / 2 : p->b_pitch;
+    auto run = [&]() -> cudaError_t {
+        cudaError_t e;
+        if (axis == 0) {
+            e = launch_xfwd<T>(p->xdct, f, nullptr, p->g, p->A, p->a_pitch, s, txh, txn, txd, nullptr, st);
+            if (e == cudaSuccess)
+                e = launch_xinv<T>(p->xdct, p->A, p->a_pitch, P, p->g, false, nullptr, nullptr, s, txh, txn, txd,
+                                   nullptr, st);
+        } else {
+            e = launch_yfwd<T>(p->ykind, reinterpret_cast<const cx<T>*>(p->A), a_cp, reinterpret_cast<cx<T>*>(p->B),
+                               b_cp, p->ycols, p->g, s, tyn, tyd, nullptr, st);
+            if (e == cudaSuccess)
+                e = launch_yinv<T>(p->ykind, reinterpret_cast<const cx<T>*>(p->B), b_cp,
+                                   reinterpret_cast<cx<T>*>(p->A), a_cp, p->ycols, p->g, s, tyn, tyd, nullptr,
+                                   nullptr, st);
+        }
+        return e;
+    };
+    cudaError_t e = run();  // warm-up (also sets the shared-memory attribute)
+    if (e != cudaSuccess) return cuda_fail(e, "autotune");
+    PPF_CK(cudaEventRecord(e0, st));
+    for (int r = 0; r < 3; ++r) {
+        e = run();
+        if (e != cudaSuccess) return cuda_fail(e, "autotune");
+    }
+    PPF_CK(cudaEventRecord(e1, st));
+    PPF_CK(cudaEventSynchronize(e1));
+    PPF_CK(cudaEventElapsedTime(ms, e0, e1));
+    return PPF_OK;
+}
+
+template <typename T>
+int tune_plan(ppf_plan* p, std::map<TuneKey, TuneChoice>& cache, const double* f, double* P, cudaStream_t st,
+              cudaEvent_t e0, cudaEvent_t e1, std::array<int, 8>& info)
+{
+    for (int axis = 0; axis < 2; ++axis) {
+        const int n = axis == 0 ? p->g.nx / 2 : p->g.ny;
+        const TuneKey key{ axis, n, axis == 0 ? (int)p->xdct : p->ykind, (int)p->elem };
+        auto it = cache.find(key);
+        if (it == cache.end()) {
+            float best = 1e30f;
+            TuneChoice pick{};
+            for (const TuneChoice& c : tune_candidates<T>(n)) {
+                float ms = 0.f;
+                int rc = time_axis<T>(p, axis, c.s, f, P, st, e0, e1, &ms);
+                if (rc != PPF_OK) return rc;
+                if (ms < best) { best = ms; pick = c; }
+            }
+            it = cache.emplace(key, pick).first;
+        }
+        const TuneChoice& c = it->second;
+        (axis == 0 ? p->sx : p->sy) = c.s;
+        info[1 + 3 * axis] = c.s.w;
+        info[2 + 3 * axis] = c.s.rt;
+        info[3 + 3 * axis] = c.order;
+    }
+    return PPF_OK;
+}
+
+double est_cost(const ppf_plan* p)
+{
+    const double cells = (double)p->g.nx * p->g.ny * p->g.nz;
+    const double passes = (p->d.precision == PPF_MIXED) ? 0.6 * (1 + p->d.max_sweeps * 1.4) : 1.0;
+    return cells * passes;
+}
+
+int batch_init(ppf_batch* b, const ppf_desc* descs, int count, int flags, int branches)
+{
+    PPF_CK(cudaGetDevice(&b->dev));
+    b->plans.assign(count, nullptr);
+    b->info.assign(count, std::array<int, 8>{});
+    for (int i = 0; i < count; ++i) {
+        int rc = validate(&descs[i]);
+        if (rc != PPF_OK) {
+            char why[sizeof(g_err)];
+            std::memcpy(why, g_err, sizeof(why));
+            return fail(rc, "problem %d: %s", i, why);
+        }
+        ppf_plan* p = new (std::nothrow) ppf_plan();
+        if (!p) return fail(PPF_ERR_NOMEM, "host allocation failed");
+        b->plans[i] = p;
+        p->own_work = false;
+        rc = plan_init(p, &descs[i]);
+        if (rc != PPF_OK) return rc;
+    }
+    // autotune on temporary buffers sized for the largest problem
+    if (flags & PPF_BATCH_AUTOTUNE) {
+        size_t fa = 0, pa = 0, aa = 0, ba = 0;
+        for (auto* p : b->plans) {
+            fa = std::max(fa, sizeof(double) * (size_t)p->g.nx * p->g.ny * p->g.nz);
+            pa = std::max(pa, sizeof(double) * (size_t)(p->g.nx + 2) * (p->g.ny + 2) * (p->g.nz + 2));
+            aa = std::max(aa, p->a_bytes);
+            ba = std::max(ba, p->b_bytes);
+        }
+        void *tf = nullptr, *tp = nullptr, *ta = nullptr, *tb = nullptr;
+        cudaStream_t st = nullptr;
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        int rc = PPF_OK;
+        if (cudaMalloc(&tf, fa) != cudaSuccess || cudaMalloc(&tp, pa) != cudaSuccess ||
+            cudaMalloc(&ta, aa) != cudaSuccess || cudaMalloc(&tb, ba) != cudaSuccess) {
+            cudaGetLastError();
+            rc = fail(PPF_ERR_NOMEM, "cannot allocate autotuning buffers");
+        }
+        if (rc == PPF_OK && (cudaMemset(tf, 0, fa) != cudaSuccess ||
+                             cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess ||
+                             cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess))
+            rc = cuda_fail(cudaGetLastError(), "autotune setup");
+        std::map<TuneKey, TuneChoice> cache;
+        for (int i = 0; i < count && rc == PPF_OK; ++i) {
+            ppf_plan* p = b->plans[i];
+            p->A = ta;
+            p->B = tb;
+            rc = (p->elem == 8) ? tune_plan<double>(p, cache, (const double*)tf, (double*)tp, st, e0, e1, b->info[i])
+                                : tune_plan<float>(p, cache, (const double*)tf, (double*)tp, st, e0, e1, b->info[i]);
+            p->A = p->B = nullptr;
+        }
+        if (st) cudaStreamSynchronize(st);
+        for (void* q : { tf, tp, ta, tb })
+            if (q) cudaFree(q);
+        if (st) cudaStreamDestroy(st);
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+        if (rc != PPF_OK) return rc;
+    }
+    // longest-first assignment to the least-loaded branch
+    int nb = branches > 0 ? branches : 8;
+    nb = std::max(1, std::min(nb, count));
+    std::vector<int> idx(count);
+    for (int i = 0; i < count; ++i) idx[i] = i;
+    std::stable_sort(idx.begin(), idx.end(),
+                     [&](int x, int y) { return est_cost(b->plans[x]) > est_cost(b->plans[y]); });
+    std::vector<double> load(nb, 0.0);
+    b->order.assign(nb, {});
+    for (int i : idx) {
+        const int br = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+        load[br] += est_cost(b->plans[i]);
+        b->order[br].push_back(i);
+        b->info[i][0] = br;
+    }
+    // one set of work buffers per branch, sized for its largest problem
+    for (int br = 0; br < nb; ++br) {
+        size_t aa = 0, ba = 0, ck = 0, pt = 0;
+        for (int i : b->order[br]) {
+            const ppf_plan* p = b->plans[i];
+            aa = std::max(aa, p->a_bytes);
+            ba = std::max(ba, p->b_bytes);
+            ck = std::max(ck, (size_t)p->ckpt_doubles);
+            pt = std::max(pt, (size_t)partials_doubles(p));
+        }
+        void *A = nullptr, *B = nullptr, *C = nullptr, *Pt = nullptr;
+        if (cudaMalloc(&A, aa) != cudaSuccess || cudaMalloc(&B, ba) != cudaSuccess ||
+            cudaMalloc(&C, sizeof(double) * std::max<size_t>(ck, 1)) != cudaSuccess ||
+            (pt && cudaMalloc(&Pt, sizeof(double) * pt) != cudaSuccess)) {
+            cudaGetLastError();
+            for (void* q : { A, B, C, Pt })
+                if (q) cudaFree(q);
+            return fail(PPF_ERR_NOMEM, "cannot allocate batch work memory for branch %d", br);
+        }
+        for (void* q : { A, B, C, Pt })
+            if (q) b->work.push_back(q);
+        for (int i : b->order[br]) {
+            ppf_plan* p = b->plans[i];
+            p->A = A;
+            p->B = B;
+            p->ckpt = (double*)C;
+            const long np = partials_doubles(p);
+            p->partials = np ? (double*)Pt : nullptr;
+            p->xinv_nblk = np / 3;
+        }
+    }
+    b->streams.assign(nb + 1, nullptr);
+    b->events.assign(nb + 1, nullptr);
+    for (int s = 0; s <= nb; ++s) {
+        PPF_CK(cudaStreamCreateWithFlags(&b->streams[s], cudaStreamNonBlocking));
+        PPF_CK(cudaEventCreateWithFlags(&b->events[s], cudaEventDisableTiming));
+    }
+    return PPF_OK;
+}
+
+int batch_capture(ppf_batch* b, const double* const* f, double* const* P, const double* const* m1,
+                  const double* const* m2, const double* const* m3, const double* const* x3)
+{
+    if (b->exec) {
+        cudaGraphExecDestroy(b->exec);
+        b->exec = nullptr;
+    }
+    cudaStream_t o = b->streams[0];
+    PPF_CK(cudaStreamBeginCapture(o, cudaStreamCaptureModeRelaxed));
+    int rc = PPF_OK;
+    cudaError_t e = cudaEventRecord(b->events[0], o);
+    const int nb = (int)b->order.size();
+    for (int br = 0; br < nb && e == cudaSuccess; ++br) e = cudaStreamWaitEvent(b->streams[1 + br], b->events[0], 0);
+    if (e != cudaSuccess) rc = cuda_fail(e, "batch capture");
+    for (int br = 0; br < nb && rc == PPF_OK; ++br)
+        for (int i : b->order[br]) {
+            rc = solve_impl(b->plans[i], f[i], P[i], m1[i], m2[i], m3[i], x3[i], b->streams[1 + br]);
+            if (rc != PPF_OK) break;
+        }
+    for (int br = 0; br < nb && rc == PPF_OK; ++br) {
+        e = cudaEventRecord(b->events[1 + br], b->streams[1 + br]);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(o, b->events[1 + br], 0);
+        if (e != cudaSuccess) rc = cuda_fail(e, "batch capture");
+    }
+    cudaGraph_t graph = nullptr;
+    e = cudaStreamEndCapture(o, &graph);
+    if (rc == PPF_OK && e != cudaSuccess) rc = cuda_fail(e, "cudaStreamEndCapture");
+    if (rc == PPF_OK) {
+        e = cudaGraphInstantiate(&b->exec, graph, 0);
+        if (e != cudaSuccess) {
+            b->exec = nullptr;
+            rc = cuda_fail(e, "cudaGraphInstantiate");
+        }
+    }
+    if (graph) cudaGraphDestroy(graph);
+    return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ppf_batch_create(const ppf_desc* descs, int count, int flags, int branches, ppf_batch** batch)
+{
+    g_err[0] = 0;
+    if (!batch) return fail(PPF_ERR_INVALID, "null batch pointer");
+    *batch = nullptr;
+    if (!descs || count < 1) return fail(PPF_ERR_INVALID, "empty batch");
+    if (flags & ~PPF_BATCH_AUTOTUNE) return fail(PPF_ERR_INVALID, "unknown batch flags 0x%x", flags);
+    ppf_batch* b = new (std::nothrow) ppf_batch();
+    if (!b) return fail(PPF_ERR_NOMEM, "host allocation failed");
+    int rc = batch_init(b, descs, count, flags, branches);
+    if (rc != PPF_OK) {
+        free_batch(b);
+        return rc;
+    }
+    *batch = b;
+    return PPF_OK;
+}
+
+int ppf_batch_destroy(ppf_batch* batch)
+{
+    if (batch) cudaDeviceSynchronize();
+    free_batch(batch);
+    return PPF_OK;
+}
+
+int ppf_batch_solve(ppf_batch* batch, const double* const* f_d, double* const* p_d, const double* const* dmx1_d,
+                    const double* const* dmx2_d, const double* const* dmx3_d, const double* const* dx3_d,
+                    void* stream)
+{
+    if (!batch) return fail(PPF_ERR_INVALID, "null batch");
+    if (!f_d || !p_d || !dmx1_d || !dmx2_d || !dmx3_d || !dx3_d) return fail(PPF_ERR_INVALID, "null pointer array");
+    int cur = -1;
+    PPF_CK(cudaGetDevice(&cur));
+    if (cur != batch->dev) return fail(PPF_ERR_STATE, "batch was created on device %d, current is %d", batch->dev, cur);
+    const int n = (int)batch->plans.size();
+    std::vector<const void*> key;
+    key.reserve(6 * (size_t)n);
+    for (int i = 0; i < n; ++i) {
+        if (!f_d[i] || !p_d[i] || !dmx1_d[i] || !dmx2_d[i] || !dmx3_d[i] || !dx3_d[i])
+            return fail(PPF_ERR_INVALID, "null array argument of problem %d", i);
+        key.insert(key.end(), { f_d[i], p_d[i], dmx1_d[i], dmx2_d[i], dmx3_d[i], dx3_d[i] });
+    }
+    if (!batch->exec || key != batch->key) {
+        int rc = batch_capture(batch, f_d, p_d, dmx1_d, dmx2_d, dmx3_d, dx3_d);
+        if (rc != PPF_OK) {
+            batch->key.clear();
+            return rc;
+        }
+        batch->key = key;
+    }
+    PPF_CK(cudaGraphLaunch(batch->exec, (cudaStream_t)stream));
+    return PPF_OK;
+}
+
+int ppf_batch_info(const ppf_batch* batch, int index, int* info)
+{
+    if (!batch || !info) return fail(PPF_ERR_INVALID, "null argument");
+    if (index < 0 || index >= (int)batch->plans.size()) return fail(PPF_ERR_INVALID, "index %d out of range", index);
+    for (int k = 0; k < 8; ++k) info[k] = batch->info[index][k];
+    info[7] = (int)batch->order.size();
+    return PPF_OK;
+}
+
+}  // extern "C"

@@ -57,6 +57,8 @@ struct FftSched {
     int n;
     int npass;
     int radix[12];
+    int w;    // lines per tile of the run-time engine (0: default width)
+    int rt;   // 1: run-time engine even where a compile-time shape exists
 };
 
 }  // namespace ppf

@@ -56,7 +56,7 @@ cudaError_t launch_xinv(bool dct, const void* in, long in_pitch, double* P, cons
 
 // blocks launch_xinv uses for geometry g (size of the partials array / 3)
 template <typename T>
-long xinv_blocks(const Geom& g);
+long xinv_blocks(const Geom& g, const FftSched& sch);
 
 // ---- Poisson TDMA along z (ppf_tdma.cu) ----
 struct ZSys {

@@ -258,10 +258,10 @@ cudaError_t launch_xfwd(bool dct, const double* f, const ResidIn* resid, const G
     ResidIn rs{};
     if (resid) rs = *resid;
     cudaError_t err = cudaSuccess;
-    with_shape<T>(nc, [&](auto sh) {
+    with_shape<T>(sch, [&](auto sh) {
         using SH = decltype(sh);
         int W, threads;
-        shape_geom<T, SH>(nc, W, threads);
+        shape_geom<T, SH>(sch, W, threads);
         if (threads > 512) { err = cudaErrorInvalidConfiguration; return; }
         const size_t smem = (size_t)nc * W * sizeof(cx<T>);
         dim3 grid((unsigned)(((long)g.ny * g.nz + W - 1) / W));
@@ -290,10 +290,10 @@ cudaError_t launch_xinv(bool dct, const void* in, long in_pitch, double* P, cons
 {
     const int nc = g.nx / 2;
     cudaError_t err = cudaSuccess;
-    with_shape<T>(nc, [&](auto sh) {
+    with_shape<T>(sch, [&](auto sh) {
         using SH = decltype(sh);
         int W, threads;
-        shape_geom<T, SH>(nc, W, threads);
+        shape_geom<T, SH>(sch, W, threads);
         if (threads > 512) { err = cudaErrorInvalidConfiguration; return; }
         const size_t smem = (size_t)nc * W * sizeof(cx<T>);
         dim3 grid((unsigned)(((long)g.ny * g.nz + W - 1) / W));
@@ -316,20 +316,20 @@ cudaError_t launch_xinv(bool dct, const void* in, long in_pitch, double* P, cons
 }
 
 template <typename T>
-long xinv_blocks(const Geom& g)
+long xinv_blocks(const Geom& g, const FftSched& sch)
 {
     long blocks = 0;
-    with_shape<T>(g.nx / 2, [&](auto sh) {
+    with_shape<T>(sch, [&](auto sh) {
         using SH = decltype(sh);
         int W, threads;
-        shape_geom<T, SH>(g.nx / 2, W, threads);
+        shape_geom<T, SH>(sch, W, threads);
         blocks = ((long)g.ny * g.nz + W - 1) / W;
     });
     return blocks;
 }
 
-template long xinv_blocks<double>(const Geom&);
-template long xinv_blocks<float>(const Geom&);
+template long xinv_blocks<double>(const Geom&, const FftSched&);
+template long xinv_blocks<float>(const Geom&, const FftSched&);
 
 #define PPF_INST(T)                                                                                        \
     template cudaError_t launch_xfwd<T>(bool, const double*, const ResidIn*, const Geom&, void*, long,     \

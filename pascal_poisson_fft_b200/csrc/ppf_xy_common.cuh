@@ -42,10 +42,14 @@ inline int ilog2i(int w)
     return l;
 }
 
+// Opt a kernel into `bytes` of dynamic shared memory.  The 48 KB default
+// covers static plus dynamic memory, and the transform kernels hold up to
+// 2.3 KB of static arrays (line tables, reduction slots), so the attribute
+// is set from 44 KB of dynamic memory on.
 template <typename K>
 cudaError_t set_smem(K kern, size_t bytes)
 {
-    if (bytes <= 48 * 1024) return cudaSuccess;
+    if (bytes <= 44 * 1024) return cudaSuccess;
     return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
@@ -71,8 +75,10 @@ inline int pick_w(int n, int& threads)
 // or 8 FP64 elements per thread), radix sequence.  Other lengths use the
 // run-time engine.
 template <typename T, typename F>
-void with_shape(int n, F&& f)
+void with_shape(const FftSched& sch, F&& f)
 {
+    const int n = sch.n;
+    if (sch.rt) { f(ShapeRT{}); return; }
     if constexpr (sizeof(T) == 8) {
         switch (n) {
             case 32:  f(ShapeCT<32, 64, 256, 8, 4>{}); return;
@@ -99,16 +105,28 @@ void with_shape(int n, F&& f)
     f(ShapeRT{});
 }
 
-// launch geometry of a shape for FFT length n (run-time shapes: pick_w)
+// launch geometry of a shape (run-time shapes: the schedule's width, else pick_w)
 template <typename T, typename SH>
-inline void shape_geom(int n, int& W, int& threads)
+inline void shape_geom(const FftSched& sch, int& W, int& threads)
 {
     if constexpr (SH::CT) {
         W = SH::W;
         threads = SH::NT;
+    } else if (sch.w > 0) {
+        W = sch.w;
+        threads = threads_for(sch.n, W);
     } else {
-        W = pick_w<T>(n, threads);
+        W = pick_w<T>(sch.n, threads);
     }
+}
+
+// a run-time width is usable: power of two, at most 128 lines, 512 threads
+// and 200 KB of shared memory
+template <typename T>
+inline bool width_ok(int n, int W)
+{
+    if (W < 1 || W > 128 || (W & (W - 1))) return false;
+    return threads_for(n, W) <= 512 && (size_t)n * W * sizeof(cx<T>) <= 200u * 1024u;
 }
 
 // FFT of the tile with the shape's engine

@@ -178,10 +178,10 @@ cudaError_t launch_yfwd(int kind, const cx<T>* in, long in_pitch, cx<T>* out, lo
                         const int* skip_flag, cudaStream_t st)
 {
     cudaError_t err = cudaSuccess;
-    with_shape<T>(g.ny, [&](auto sh) {
+    with_shape<T>(sch, [&](auto sh) {
         using SH = decltype(sh);
         int W, threads;
-        shape_geom<T, SH>(g.ny, W, threads);
+        shape_geom<T, SH>(sch, W, threads);
         if (threads > 512) { err = cudaErrorInvalidConfiguration; return; }
         const size_t smem = (size_t)g.ny * W * sizeof(cx<T>);
         dim3 grid((unsigned)((ncols + W - 1) / W), (unsigned)g.nz);
@@ -205,10 +205,10 @@ cudaError_t launch_yinv(int kind, const cx<T>* in, long in_pitch, cx<T>* out, lo
                         const double* dc_shift, const int* skip_flag, cudaStream_t st)
 {
     cudaError_t err = cudaSuccess;
-    with_shape<T>(g.ny, [&](auto sh) {
+    with_shape<T>(sch, [&](auto sh) {
         using SH = decltype(sh);
         int W, threads;
-        shape_geom<T, SH>(g.ny, W, threads);
+        shape_geom<T, SH>(sch, W, threads);
         if (threads > 512) { err = cudaErrorInvalidConfiguration; return; }
         const size_t smem = (size_t)g.ny * W * sizeof(cx<T>);
         dim3 grid((unsigned)((ncols + W - 1) / W), (unsigned)g.nz);

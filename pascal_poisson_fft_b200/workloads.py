@@ -151,6 +151,61 @@ def config3_field(p: Problem, seed: int, modes: int = 48, noise: float = 1e-3, d
     return f
 
 
+C4_XY = (48, 64, 96, 128, 160, 192, 256, 320, 384)
+C4_Z = (32, 64, 128, 256)
+
+
+def config4(seed: int = 4, count: int = 96, generate: bool = True, device=None):
+    """Batched uneven problems: Nx, Ny drawn from C4_XY (radix 2, 3, 5), Nz
+    from C4_Z, periodic or Neumann (DCT) per problem in x and y, Neumann z,
+    uniform z spacing, on [0,2pi)^2 x [0,1].  Right-hand sides are seeded
+    Gaussian fields smoothed by a 3-point (1/4, 1/2, 1/4) filter along each
+    axis (wrapping on periodic axes, mirrored at walls), mean removed.
+    With `device`, fields are torch tensors made there."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    probs = []
+    for k in range(count):
+        nx, ny = int(rng.choice(C4_XY)), int(rng.choice(C4_XY))
+        nz = int(rng.choice(C4_Z))
+        pbc = (bool(rng.integers(2)), bool(rng.integers(2)), False)
+        probs.append(build_metrics(Problem(f"c4_{k}", nx, ny, nz, TWO_PI, TWO_PI, 1.0, pbc, 0.0)))
+    if generate:
+        for k, p in enumerate(probs):
+            p.f = config4_field(p, seed * 1000 + k, device)
+    return probs
+
+
+def config4_field(p: Problem, seed: int, device=None):
+    """The config-4 right-hand side of one problem (numpy, or torch on `device`)."""
+    if device is None:
+        g = np.random.Generator(np.random.PCG64(seed)).standard_normal(p.shape)
+        for ax, per in ((2, p.pbc[0]), (1, p.pbc[1]), (0, p.pbc[2])):
+            lo = np.roll(g, 1, axis=ax)
+            hi = np.roll(g, -1, axis=ax)
+            if not per:   # mirror at the walls: the outside neighbour is the cell itself
+                idx = [slice(None)] * 3
+                idx[ax] = 0
+                lo[tuple(idx)] = g[tuple(idx)]
+                idx[ax] = -1
+                hi[tuple(idx)] = g[tuple(idx)]
+            g = 0.25 * lo + 0.5 * g + 0.25 * hi
+        return remove_volume_mean(g, p.metrics["dx3"])
+    import torch
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    g = torch.randn(p.shape, dtype=torch.float64, device=device, generator=gen)
+    for ax, per in ((2, p.pbc[0]), (1, p.pbc[1]), (0, p.pbc[2])):
+        lo = torch.roll(g, 1, dims=ax)
+        hi = torch.roll(g, -1, dims=ax)
+        if not per:
+            lo.select(ax, 0).copy_(g.select(ax, 0))
+            hi.select(ax, g.shape[ax] - 1).copy_(g.select(ax, g.shape[ax] - 1))
+        g = 0.25 * lo + 0.5 * g + 0.25 * hi
+    w = torch.as_tensor(p.metrics["dx3"][1:p.n3m + 1], dtype=torch.float64, device=device)
+    g -= (g.mean(dim=(1, 2)) * w).sum() / w.sum()
+    return g
+
+
 def config5(seed: int = 5, n1m: int = 256, n2m: int = 256, n3m: int = 128, beta: float = 2.0,
             modes: int = 48, noise: float = 1e-3):
     """Differentiation workload: periodic x,y, tanh z (beta); the right-hand

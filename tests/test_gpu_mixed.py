@@ -61,3 +61,15 @@ def test_mixed_deterministic():
     P1, plan = gpu_solve(p, precision=PPF_MIXED, max_sweeps=2, return_plan=True)
     P2 = gpu_solve(p, plan=plan)
     assert np.array_equal(P1, P2)
+
+
+def test_fp32_768x768x384_radix3():
+    """The FP32 single-solve throughput configuration (768x768x384, radix
+    3*2^k): the mixed path within 1e-10 of the FP64 solve, and a single FP32
+    solve within 2e-4 (its error grows with the grid: ~7e-5 here)."""
+    p = W.config3(n1m=768, n2m=768, n3m=384, generate=False)
+    import torch
+    p.f = W.config3_field(p, 3, device=torch.device("cuda", 0)).cpu().numpy()
+    P64 = gpu_solve(p)
+    assert rel_l2(gpu_solve(p, precision=PPF_MIXED, max_sweeps=3), P64) < TOL_MIXED
+    assert rel_l2(gpu_solve(p, precision=PPF_FP32), P64) < 2e-4

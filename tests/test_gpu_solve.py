@@ -26,6 +26,15 @@ def test_golden_fixture_cases():
         assert rel_l2(P, g[f"{i}_P"]) < TOL64, (i, (n1, n2, n3), (p1, p2, p3))
 
 
+@pytest.mark.parametrize("shape", [(768, 16, 6), (16, 768, 6), (1024, 8, 4), (8, 1024, 4), (640, 20, 5)])
+@pytest.mark.parametrize("pbc", [(1, 1, 0), (0, 0, 0)])
+def test_fp64_long_lines(shape, pbc):
+    """Longest transform lines (tiles of 48 KB and more of shared memory)."""
+    rng = np.random.default_rng(hash((shape, pbc)) & 0xffff)
+    p = W.random_problem(rng, *shape, pbc, beta=1.0)
+    assert rel_l2(gpu_solve(p), oracle_solve(p)) < TOL64
+
+
 @pytest.mark.parametrize("shape", [(16, 12, 10), (32, 32, 32), (48, 40, 24), (96, 80, 33), (40, 30, 100),
                                    (20, 24, 513)])
 @pytest.mark.parametrize("pbc", [(1, 1, 0), (0, 0, 0), (0, 1, 0), (1, 0, 0), (1, 1, 1)])
