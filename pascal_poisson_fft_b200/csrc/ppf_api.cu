@@ -117,6 +117,9 @@ struct ppf_plan {
     double* ckpt = nullptr;      // Thomas checkpoints of the z solve
     long ckpt_doubles = 0;
     bool own_work = true;        // A, B, ckpt, partials belong to the plan (not to a batch)
+    // auxiliary stream of the FP64 low-|k| z solves of the mixed and FP32 paths
+    cudaStream_t aux = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     void* tw = nullptr;        // twiddle tables (type T)
     size_t tw_off[5] = {};     // element offsets: x half, x n, x dct, y n, y dct
     FftSched sx{}, sy{};
@@ -185,6 +188,9 @@ void free_plan(ppf_plan* p)
                      p->f_dev, p->p_dev, p->m_dev, p->adj_W, p->adj_red };
     for (void* q : ptrs)
         if (q) cudaFree(q);
+    if (p->aux) cudaStreamDestroy(p->aux);
+    if (p->ev_fork) cudaEventDestroy(p->ev_fork);
+    if (p->ev_join) cudaEventDestroy(p->ev_join);
     if (p->own_work) {
         void* work[] = { p->A, p->B, p->partials, p->ckpt };
         for (void* q : work)
@@ -286,6 +292,11 @@ int plan_init(ppf_plan* p, const ppf_desc* d)
     PPF_CK(cudaMemset(p->scal, 0, sizeof(double) * 8));
     PPF_CK(cudaMemset(p->flags, 0, sizeof(int) * 4));
     p->ckpt_doubles = tdma_z_ckpt_doubles(nz, p->b_pitch * (long)p->my, p->g.pz);
+    if (p->elem == 4) {
+        PPF_CK(cudaStreamCreateWithFlags(&p->aux, cudaStreamNonBlocking));
+        PPF_CK(cudaEventCreateWithFlags(&p->ev_fork, cudaEventDisableTiming));
+        PPF_CK(cudaEventCreateWithFlags(&p->ev_join, cudaEventDisableTiming));
+    }
     PPF_CK(cudaMemcpy(p->lamx, lx.data(), sizeof(double) * p->mx, cudaMemcpyHostToDevice));
     PPF_CK(cudaMemcpy(p->lamy, ly.data(), sizeof(double) * p->my, cudaMemcpyHostToDevice));
     int rc = (p->elem == 8) ? upload_twiddles<double>(p) : upload_twiddles<float>(p);
@@ -355,16 +366,18 @@ int run_pass(ppf_plan* p, const double* f, double* P, bool resid, bool accumulat
     z.dc_shift = p->scal + 4;
     z.cyclic = p->g.pz;
     z.ckpt = p->ckpt;
-    e = p->cplx ? launch_tdma_z<T, true>(p->B, z, skip, p->flags + 2, st)
-                : launch_tdma_z<T, false>(p->B, z, skip, p->flags + 2, st);
+    const ZStreams zs{ st, p->aux, p->ev_fork, p->ev_join };
+    e = p->cplx ? launch_tdma_z<T, true>(p->B, z, skip, p->flags + 2, zs)
+                : launch_tdma_z<T, false>(p->B, z, skip, p->flags + 2, zs);
     if (e != cudaSuccess) return cuda_fail(e, "z tridiagonal");
     mark(p, 3, st);
     e = launch_yinv<T>(p->ykind, reinterpret_cast<const cx<T>*>(p->B), b_cp, reinterpret_cast<cx<T>*>(p->A), a_cp,
                        p->ycols, p->g, p->sy, tyn, tyd, p->scal + 4, skip, st);
     if (e != cudaSuccess) return cuda_fail(e, "y inverse");
     mark(p, 4, st);
-    e = launch_xinv<T>(p->xdct, p->A, p->a_pitch, P, p->g, accumulate, p->partials, p->scal + 5, p->sx,
-                       txh, txn, txd, skip, st);
+    // the mixed path keeps the stencil's ghost cells current for its residual
+    e = launch_xinv<T>(p->xdct, p->A, p->a_pitch, P, p->g, accumulate, p->d.precision == PPF_MIXED, p->partials,
+                       p->scal + 5, p->sx, txh, txn, txd, skip, st);
     if (e != cudaSuccess) return cuda_fail(e, "x inverse");
     mark(p, 5, st);
     return PPF_OK;
@@ -972,8 +985,8 @@ int time_axis(ppf_plan* p, int axis, const FftSched& s, const double* f, double*
         if (axis == 0) {
             e = launch_xfwd<T>(p->xdct, f, nullptr, p->g, p->A, p->a_pitch, s, txh, txn, txd, nullptr, st);
             if (e == cudaSuccess)
-                e = launch_xinv<T>(p->xdct, p->A, p->a_pitch, P, p->g, false, nullptr, nullptr, s, txh, txn, txd,
-                                   nullptr, st);
+                e = launch_xinv<T>(p->xdct, p->A, p->a_pitch, P, p->g, false, false, nullptr, nullptr, s, txh,
+                                   txn, txd, nullptr, st);
         } else {
             e = launch_yfwd<T>(p->ykind, reinterpret_cast<const cx<T>*>(p->A), a_cp, reinterpret_cast<cx<T>*>(p->B),
                                b_cp, p->ycols, p->g, s, tyn, tyd, nullptr, st);

@@ -21,14 +21,9 @@ struct ResidIn {
     double ix2, iy2;      // 1/dx^2, 1/dy^2 (uniform x, y)
 };
 
-// Accumulation options of the x-inverse pass.
-struct AccumOut {
-    double* norms;        // [0] += sum du^2, [1] += sum u_new^2 (may be null)
-};
-
 enum YKind { Y_C2C = 0, Y_CDCT = 1, Y_RPAIR = 2 };
 
-// ---- launchers (defined in ppf_xy.cu) ----
+// ---- transform launchers (ppf_x.cu, ppf_y.cu) ----
 template <typename T>
 cudaError_t launch_xfwd(bool dct, const double* f, const ResidIn* resid, const Geom& g,
                         void* out, long out_pitch, const FftSched& sch,
@@ -50,8 +45,8 @@ cudaError_t launch_yinv(int kind, const cx<T>* in, long in_pitch, cx<T>* out, lo
 // partials (optional): per-block [sum du^2, sum u^2, sum u], 3 doubles per block.
 template <typename T>
 cudaError_t launch_xinv(bool dct, const void* in, long in_pitch, double* P, const Geom& g,
-                        bool accumulate, double* partials, const double* mean_prev, const FftSched& sch,
-                        const cx<T>* tw_half, const cx<T>* tw_n, const cx<T>* tw_dct,
+                        bool accumulate, bool stencil_ghosts, double* partials, const double* mean_prev,
+                        const FftSched& sch, const cx<T>* tw_half, const cx<T>* tw_n, const cx<T>* tw_dct,
                         const int* skip_flag, cudaStream_t st);
 
 // blocks launch_xinv uses for geometry g (size of the partials array / 3)
@@ -79,8 +74,17 @@ struct ZSys {
 // doubles of checkpoint memory the z solve needs
 long tdma_z_ckpt_doubles(int nz, long plane, int cyclic);
 
+// streams of the z solve: the FP32 bulk runs on st; the FP64 low-|k|
+// systems run on aux (forked from and joined back to st through the two
+// events) when aux is given, else on st after the bulk
+struct ZStreams {
+    cudaStream_t st;
+    cudaStream_t aux;
+    cudaEvent_t fork, join;
+};
+
 template <typename T, bool CPLX>
-cudaError_t launch_tdma_z(void* data, const ZSys& z, const int* skip_flag, int* err_flag, cudaStream_t st);
+cudaError_t launch_tdma_z(void* data, const ZSys& z, const int* skip_flag, int* err_flag, const ZStreams& zs);
 
 cudaError_t launch_zcoef(const double* dx3, const double* dmx3, int nz, double* am, double* ap,
                          double* dzmax2, cudaStream_t st);

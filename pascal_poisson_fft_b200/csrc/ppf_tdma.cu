@@ -383,32 +383,48 @@ long tdma_z_ckpt_doubles(int nz, long plane, int cyclic)
 
 namespace {
 template <bool CPLX, bool CYC>
-void launch_z(double*, const ZSys& z, void* data, const int* skip, int* err, cudaStream_t st)
+cudaError_t launch_z(double*, const ZSys& z, void* data, const int* skip, int* err, const ZStreams& zs)
 {
     dim3 grid((unsigned)((z.plane + TPB - 1) / TPB));  // pitch * my systems incl. padding columns
-    k_thomas_z<double, Exact, CPLX, 0, CYC><<<grid, TPB, 0, st>>>(data, z, skip, err);
+    k_thomas_z<double, Exact, CPLX, 0, CYC><<<grid, TPB, 0, zs.st>>>(data, z, skip, err);
+    return cudaGetLastError();
 }
+// FP32 data: the bulk in FP32 and, concurrently on the auxiliary stream when
+// one is given, the few low-|k| systems in FP64 (a short grid-wide launch
+// whose duration is the latency of its long FP64 Thomas chains)
 template <bool CPLX, bool CYC>
-void launch_z(float*, const ZSys& z, void* data, const int* skip, int* err, cudaStream_t st)
+cudaError_t launch_z(float*, const ZSys& z, void* data, const int* skip, int* err, const ZStreams& zs)
 {
     dim3 grid((unsigned)((z.plane + TPB - 1) / TPB));
-    k_thomas_z<float, Fast, CPLX, 1, CYC><<<grid, TPB, 0, st>>>(data, z, skip, err);
-    k_thomas_z<float, Exact, CPLX, 2, CYC><<<grid, TPB, 0, st>>>(data, z, skip, err);
+    cudaStream_t lo = zs.st;
+    if (zs.aux) {
+        cudaError_t e = cudaEventRecord(zs.fork, zs.st);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(zs.aux, zs.fork, 0);
+        if (e != cudaSuccess) return e;
+        lo = zs.aux;
+    }
+    k_thomas_z<float, Exact, CPLX, 2, CYC><<<grid, TPB, 0, lo>>>(data, z, skip, err);
+    k_thomas_z<float, Fast, CPLX, 1, CYC><<<grid, TPB, 0, zs.st>>>(data, z, skip, err);
+    if (zs.aux) {
+        cudaError_t e = cudaEventRecord(zs.join, zs.aux);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(zs.st, zs.join, 0);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaGetLastError();
 }
 }  // namespace
 
 template <typename T, bool CPLX>
-cudaError_t launch_tdma_z(void* data, const ZSys& z, const int* skip_flag, int* err_flag, cudaStream_t st)
+cudaError_t launch_tdma_z(void* data, const ZSys& z, const int* skip_flag, int* err_flag, const ZStreams& zs)
 {
-    if (z.cyclic) launch_z<CPLX, true>((T*)nullptr, z, data, skip_flag, err_flag, st);
-    else          launch_z<CPLX, false>((T*)nullptr, z, data, skip_flag, err_flag, st);
-    return cudaGetLastError();
+    if (z.cyclic) return launch_z<CPLX, true>((T*)nullptr, z, data, skip_flag, err_flag, zs);
+    return launch_z<CPLX, false>((T*)nullptr, z, data, skip_flag, err_flag, zs);
 }
 
-template cudaError_t launch_tdma_z<double, true>(void*, const ZSys&, const int*, int*, cudaStream_t);
-template cudaError_t launch_tdma_z<double, false>(void*, const ZSys&, const int*, int*, cudaStream_t);
-template cudaError_t launch_tdma_z<float, true>(void*, const ZSys&, const int*, int*, cudaStream_t);
-template cudaError_t launch_tdma_z<float, false>(void*, const ZSys&, const int*, int*, cudaStream_t);
+template cudaError_t launch_tdma_z<double, true>(void*, const ZSys&, const int*, int*, const ZStreams&);
+template cudaError_t launch_tdma_z<double, false>(void*, const ZSys&, const int*, int*, const ZStreams&);
+template cudaError_t launch_tdma_z<float, true>(void*, const ZSys&, const int*, int*, const ZStreams&);
+template cudaError_t launch_tdma_z<float, false>(void*, const ZSys&, const int*, int*, const ZStreams&);
 
 // --------------------------------------------------------------------------
 // Coefficient-array solves, element (sys, row) at [row * n_sys + sys].

@@ -38,28 +38,59 @@ __global__ void __launch_bounds__(512) k_xfwd(const double* __restrict__ f, Resi
     const long nlines = (long)g.ny * g.nz;
     const long line0 = (long)blockIdx.x * W;
     const int E = nc << lgW;
-    // (y, z) of each line of the tile, computed once (no per-element division)
-    __shared__ int line_j[MAXW], line_k[MAXW];
+    // per line of the tile: offset of its first cell in the ghosted P and
+    // the z coefficients of its level (no per-element division)
+    __shared__ long line_c[MAXW];
+    __shared__ double line_am[MAXW], line_ap[MAXW];
     if (RESID) {
         for (int l = threadIdx.x; l < W; l += NTH) {
             const long line = line0 + l;
-            line_j[l] = (int)(line % g.ny);
-            line_k[l] = (int)(line / g.ny);
+            const long j = line % g.ny, k = line / g.ny;
+            line_c[l] = 1 + (j + 1) * g.pstride_y + (k + 1) * g.pstride_z;
+            line_am[l] = (k < g.nz) ? rs.am[k] : 0.0;
+            line_ap[l] = (k < g.nz) ? rs.ap[k] : 0.0;
         }
         __syncthreads();
     }
+    // f and P are 16-byte aligned (cudaMalloc'd arrays): pairs load as one vector
+    const bool vec = ((reinterpret_cast<size_t>(f) | reinterpret_cast<size_t>(rs.P)) & 15) == 0;
+    const long sy = g.pstride_y, sz = g.pstride_z;
 
     for (int e = threadIdx.x; e < E; e += NTH) {
         const int l = e / nc, n = e - l * nc;
         const long line = line0 + l;
         cx<T> z = mk<T>((T)0, (T)0);
         if (line < nlines) {
-            const double* fl = f + line * nx;
-            double a = fl[2 * n], b = fl[2 * n + 1];
+            const double* fl = f + line * nx + 2 * n;
+            double a, b;
+            if (vec) {
+                const double2 fv = __ldg(reinterpret_cast<const double2*>(fl));
+                a = fv.x;
+                b = fv.y;
+            } else {
+                a = fl[0];
+                b = fl[1];
+            }
             if (RESID) {
-                const int j = line_j[l], k = line_k[l];
-                a -= lap_at(rs, g, 2 * n, j, k);
-                b -= lap_at(rs, g, 2 * n + 1, j, k);
+                // f - L_h u at cells 2n and 2n+1.  The ghost cells hold the
+                // stencil's neighbours (periodic copies or wall mirrors, written
+                // by the previous x-inverse pass), so no index wraps here.
+                const double* c = rs.P + line_c[l] + 2 * n;   // c[0] = u(2n), odd offset
+                double xm, u0, u1, xp;
+                if (vec) {
+                    const double2 lo = __ldg(reinterpret_cast<const double2*>(c - 1));
+                    const double2 hi = __ldg(reinterpret_cast<const double2*>(c + 1));
+                    xm = lo.x; u0 = lo.y; u1 = hi.x; xp = hi.y;
+                } else {
+                    xm = c[-1]; u0 = c[0]; u1 = c[1]; xp = c[2];
+                }
+                const double ym0 = c[-sy], ym1 = c[1 - sy], yp0 = c[sy], yp1 = c[1 + sy];
+                const double zm0 = c[-sz], zm1 = c[1 - sz], zp0 = c[sz], zp1 = c[1 + sz];
+                const double am = line_am[l], ap = line_ap[l];
+                a -= (xm - 2.0 * u0 + u1) * rs.ix2 + (ym0 - 2.0 * u0 + yp0) * rs.iy2 + am * (zm0 - u0) +
+                     ap * (zp0 - u0);
+                b -= (u0 - 2.0 * u1 + xp) * rs.ix2 + (ym1 - 2.0 * u1 + yp1) * rs.iy2 + am * (zm1 - u1) +
+                     ap * (zp1 - u1);
             }
             z = mk<T>((T)a, (T)b);
         }
@@ -140,7 +171,7 @@ __global__ void __launch_bounds__(512) k_xfwd(const double* __restrict__ f, Resi
 // interior of the ghosted FP64 output.  ACC: u <- (u - mean_prev) + du.
 // partials (optional): per-block [sum du^2, sum u^2, sum u].
 // --------------------------------------------------------------------------
-template <typename T, bool DCT, bool ACC, typename SH>
+template <typename T, bool DCT, bool ACC, bool GHOST, typename SH>
 __global__ void __launch_bounds__(512) k_xinv(const void* __restrict__ in_, long in_pitch, double* __restrict__ P,
                                                Geom g, double* __restrict__ partials,
                                                const double* __restrict__ mean_prev, FftSched sch, int Wrt,
@@ -191,12 +222,25 @@ __global__ void __launch_bounds__(512) k_xinv(const void* __restrict__ in_, long
         }
         s[sidx<T>(k, l, W)] = Z;
     }
-    // ghosted-output offset of each line of the tile (no per-element division)
-    __shared__ long line_base[MAXW];
+    // ghosted-output offset of each line of the tile, and (GHOST) the offsets
+    // of the ghost lines its values are copied to (0: none)
+    __shared__ long line_base[MAXW], line_gy[MAXW], line_gz[MAXW];
     for (int l = threadIdx.x; l < W; l += NTH) {
         const long line = line0 + l;
         const long j = line % g.ny, k = line / g.ny;
         line_base[l] = 1 + (j + 1) * g.pstride_y + (k + 1) * g.pstride_z;
+        if (GHOST) {
+            // y: periodic copy to the opposite ghost row, or mirror at the wall
+            long gy = 0;
+            if (j == 0) gy = g.py ? (long)g.ny * g.pstride_y : -g.pstride_y;
+            else if (j == g.ny - 1) gy = g.py ? -(long)g.ny * g.pstride_y : g.pstride_y;
+            // z: any finite value (the wall coefficients am_1, ap_n3m are 0)
+            long gz = 0;
+            if (k == 0) gz = -g.pstride_z;
+            else if (k == g.nz - 1) gz = g.pstride_z;
+            line_gy[l] = gy;
+            line_gz[l] = gz;
+        }
     }
     __syncthreads();
     tile_fft<T, true, SH>(s, sch, W, lgW, tw_half);
@@ -218,6 +262,15 @@ __global__ void __launch_bounds__(512) k_xinv(const void* __restrict__ in_, long
         // iterate (the residual cannot see constants, so the gauge is kept here)
         const double un = ACC ? (P[o] - mprev) + x : x;
         P[o] = un;
+        if (GHOST) {
+            // stencil ghosts for the next residual (the reference's ghost
+            // update overwrites them after the last sweep)
+            if (i == 0) P[o + (g.px ? nx : -1)] = un;
+            if (i == nx - 1) P[o + (g.px ? -nx : 1)] = un;
+            const long gy = line_gy[l], gz = line_gz[l];
+            if (gy) P[o + gy] = un;
+            if (gz) P[o + gz] = un;
+        }
         if (partials) {
             acc_du += x * x;
             acc_u += un * un;
@@ -285,8 +338,9 @@ cudaError_t launch_xfwd(bool dct, const double* f, const ResidIn* resid, const G
 
 template <typename T>
 cudaError_t launch_xinv(bool dct, const void* in, long in_pitch, double* P, const Geom& g, bool accumulate,
-                        double* partials, const double* mean_prev, const FftSched& sch, const cx<T>* tw_half,
-                        const cx<T>* tw_n, const cx<T>* tw_dct, const int* skip_flag, cudaStream_t st)
+                        bool stencil_ghosts, double* partials, const double* mean_prev, const FftSched& sch,
+                        const cx<T>* tw_half, const cx<T>* tw_n, const cx<T>* tw_dct, const int* skip_flag,
+                        cudaStream_t st)
 {
     const int nc = g.nx / 2;
     cudaError_t err = cudaSuccess;
@@ -304,12 +358,18 @@ cudaError_t launch_xinv(bool dct, const void* in, long in_pitch, double* P, cons
                                               tw_n, tw_dct, skip_flag);
             err = cudaGetLastError();
         };
-        if (dct) {
-            if (accumulate) go(k_xinv<T, true, true, SH>);
-            else go(k_xinv<T, true, false, SH>);
+        if (stencil_ghosts) {
+            if (dct) {
+                if (accumulate) go(k_xinv<T, true, true, true, SH>);
+                else go(k_xinv<T, true, false, true, SH>);
+            } else {
+                if (accumulate) go(k_xinv<T, false, true, true, SH>);
+                else go(k_xinv<T, false, false, true, SH>);
+            }
+        } else if (dct) {
+            go(k_xinv<T, true, false, false, SH>);
         } else {
-            if (accumulate) go(k_xinv<T, false, true, SH>);
-            else go(k_xinv<T, false, false, SH>);
+            go(k_xinv<T, false, false, false, SH>);
         }
     });
     return err;
@@ -335,9 +395,9 @@ template long xinv_blocks<float>(const Geom&, const FftSched&);
     template cudaError_t launch_xfwd<T>(bool, const double*, const ResidIn*, const Geom&, void*, long,     \
                                         const FftSched&, const cx<T>*, const cx<T>*, const cx<T>*,         \
                                         const int*, cudaStream_t);                                         \
-    template cudaError_t launch_xinv<T>(bool, const void*, long, double*, const Geom&, bool, double*,      \
-                                        const double*, const FftSched&, const cx<T>*, const cx<T>*,        \
-                                        const cx<T>*, const int*, cudaStream_t);
+    template cudaError_t launch_xinv<T>(bool, const void*, long, double*, const Geom&, bool, bool,        \
+                                        double*, const double*, const FftSched&, const cx<T>*,             \
+                                        const cx<T>*, const cx<T>*, const int*, cudaStream_t);
 PPF_INST(double)
 PPF_INST(float)
 #undef PPF_INST

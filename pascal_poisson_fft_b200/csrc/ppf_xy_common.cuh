@@ -5,36 +5,6 @@
 
 namespace ppf {
 
-// L_h u at cell (i, j, k): 3-point x and y second differences (periodic
-// wrap or mirror at a Neumann wall, uniform spacing) plus the finite-volume
-// z stencil am (u_{k-1} - u) + ap (u_{k+1} - u) -- the operator the
-// transforms and the z solve invert.
-__device__ __forceinline__ double lap_at(const ResidIn& r, const Geom& g, int i, int j, int k)
-{
-    const double* P = r.P;
-    const long base = (long)(i + 1) + (long)(j + 1) * g.pstride_y + (long)(k + 1) * g.pstride_z;
-    const double u = P[base];
-    double uxm, uxp, uym, uyp, uzm, uzp;
-    if (g.px) {
-        uxm = P[base + (i == 0 ? (g.nx - 1) : -1)];
-        uxp = P[base + (i == g.nx - 1 ? -(g.nx - 1) : 1)];
-    } else {
-        uxm = (i == 0) ? u : P[base - 1];
-        uxp = (i == g.nx - 1) ? u : P[base + 1];
-    }
-    if (g.py) {
-        uym = P[base + (j == 0 ? (long)(g.ny - 1) * g.pstride_y : -g.pstride_y)];
-        uyp = P[base + (j == g.ny - 1 ? -(long)(g.ny - 1) * g.pstride_y : g.pstride_y)];
-    } else {
-        uym = (j == 0) ? u : P[base - g.pstride_y];
-        uyp = (j == g.ny - 1) ? u : P[base + g.pstride_y];
-    }
-    uzm = (k == 0) ? u : P[base - g.pstride_z];
-    uzp = (k == g.nz - 1) ? u : P[base + g.pstride_z];
-    const double am = r.am[k], ap = r.ap[k];
-    return (uxm - 2.0 * u + uxp) * r.ix2 + (uym - 2.0 * u + uyp) * r.iy2 + am * (uzm - u) + ap * (uzp - u);
-}
-
 inline int ilog2i(int w)
 {
     int l = 0;
@@ -44,12 +14,12 @@ inline int ilog2i(int w)
 
 // Opt a kernel into `bytes` of dynamic shared memory.  The 48 KB default
 // covers static plus dynamic memory, and the transform kernels hold up to
-// 2.3 KB of static arrays (line tables, reduction slots), so the attribute
-// is set from 44 KB of dynamic memory on.
+// 4 KB of static arrays (line tables, reduction slots), so the attribute
+// is set from 40 KB of dynamic memory on.
 template <typename K>
 cudaError_t set_smem(K kern, size_t bytes)
 {
-    if (bytes <= 44 * 1024) return cudaSuccess;
+    if (bytes <= 40 * 1024) return cudaSuccess;
     return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
