@@ -376,8 +376,10 @@ int run_pass(ppf_plan* p, const double* f, double* P, bool resid, bool accumulat
     if (e != cudaSuccess) return cuda_fail(e, "y inverse");
     mark(p, 4, st);
     // the mixed path keeps the stencil's ghost cells current for its residual
+    long nblk = 0;
     e = launch_xinv<T>(p->xdct, p->A, p->a_pitch, P, p->g, accumulate, p->d.precision == PPF_MIXED, p->partials,
-                       p->scal + 5, p->sx, txh, txn, txd, skip, st);
+                       p->scal + 5, p->sx, txh, txn, txd, skip, st, &nblk);
+    if (p->partials) p->xinv_nblk = nblk;  // the refinement gate reduces these blocks' partial sums
     if (e != cudaSuccess) return cuda_fail(e, "x inverse");
     mark(p, 5, st);
     return PPF_OK;

@@ -52,6 +52,30 @@ __device__ __forceinline__ int sidx(int n, int l, int W)
     return n * W + (l ^ (n & (W - 1) & (G - 1)));
 }
 
+// Asynchronous global -> shared copies (cp.async): one element per call,
+// completion tracked per thread by commit groups.
+__device__ __forceinline__ void cp_async_elem(cx<float>* dst, const cx<float>* src)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_elem(cx<double>* dst, const cx<double>* src)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+// wait until at most N of this thread's most recent groups are pending
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// Bulk prefetch of `bytes` (a multiple of 16) at a 16-byte aligned global
+// address into L2.
+__device__ __forceinline__ void prefetch_l2(const void* p, unsigned bytes)
+{
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(p), "r"(bytes) : "memory");
+}
+
 // Per-axis FFT schedule: complex length n = prod(radix[0..npass)).
 struct FftSched {
     int n;

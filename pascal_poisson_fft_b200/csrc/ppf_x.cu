@@ -191,6 +191,14 @@ __global__ void __launch_bounds__(512) k_xinv(const void* __restrict__ in_, long
     const long nlines = (long)g.ny * g.nz;
     const long line0 = (long)blockIdx.x * W;
     const int E = nc << lgW;
+    // the P rows this tile updates are fetched into L2 in bulk now, so that
+    // the read-modify-write after the transform finds them there
+    if (ACC && threadIdx.x < W && (reinterpret_cast<size_t>(P) & 15) == 0) {
+        const long line = line0 + threadIdx.x;
+        if (line < nlines)
+            prefetch_l2(P + (line % g.ny + 1) * g.pstride_y + (line / g.ny + 1) * g.pstride_z,
+                        (unsigned)((nx + 2) * sizeof(double)));
+    }
 
     for (int e = threadIdx.x; e < E; e += NTH) {
         const int l = e / nc, k = e - l * nc;
@@ -340,7 +348,7 @@ template <typename T>
 cudaError_t launch_xinv(bool dct, const void* in, long in_pitch, double* P, const Geom& g, bool accumulate,
                         bool stencil_ghosts, double* partials, const double* mean_prev, const FftSched& sch,
                         const cx<T>* tw_half, const cx<T>* tw_n, const cx<T>* tw_dct, const int* skip_flag,
-                        cudaStream_t st)
+                        cudaStream_t st, long* blocks_used)
 {
     const int nc = g.nx / 2;
     cudaError_t err = cudaSuccess;
@@ -351,6 +359,7 @@ cudaError_t launch_xinv(bool dct, const void* in, long in_pitch, double* P, cons
         if (threads > 512) { err = cudaErrorInvalidConfiguration; return; }
         const size_t smem = (size_t)nc * W * sizeof(cx<T>);
         dim3 grid((unsigned)(((long)g.ny * g.nz + W - 1) / W));
+        if (blocks_used) *blocks_used = grid.x;
         auto go = [&](auto kern) {
             err = set_smem(kern, smem);
             if (err != cudaSuccess) return;
@@ -397,7 +406,7 @@ template long xinv_blocks<float>(const Geom&, const FftSched&);
                                         const int*, cudaStream_t);                                         \
     template cudaError_t launch_xinv<T>(bool, const void*, long, double*, const Geom&, bool, bool,        \
                                         double*, const double*, const FftSched&, const cx<T>*,             \
-                                        const cx<T>*, const cx<T>*, const int*, cudaStream_t);
+                                        const cx<T>*, const cx<T>*, const int*, cudaStream_t, long*);
 PPF_INST(double)
 PPF_INST(float)
 #undef PPF_INST

@@ -3,6 +3,9 @@
 #include "ppf_fft.cuh"
 #include "ppf_kernels.cuh"
 
+#include <algorithm>
+#include <mutex>
+
 namespace ppf {
 
 inline int ilog2i(int w)
@@ -105,6 +108,40 @@ __device__ __forceinline__ void tile_fft(cx<T>* s, const FftSched& sch, int W, i
 {
     if constexpr (SH::CT) SH::template fft<T, INV>(s, tw);
     else fft_tile<T, INV>(s, sch, W, lgW, tw);
+}
+
+// grid of a persistent kernel: resident CTAs on every SM, at most one per
+// tile.  Resident CTAs are computed once per kernel and device.
+template <typename K>
+cudaError_t persistent_grid(K kern, int threads, size_t smem, long tiles, unsigned* grid)
+{
+    struct Slot { const void* fn; int dev; int slots; };
+    static Slot cache[256];
+    static int used = 0;
+    static std::mutex mu;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const void* fn = reinterpret_cast<const void*>(kern);
+    int slots = 0;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        for (int i = 0; i < used; ++i)
+            if (cache[i].fn == fn && cache[i].dev == dev) { slots = cache[i].slots; break; }
+    }
+    if (slots == 0) {
+        int sms = 0, per = 0;
+        e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, threads, smem);
+        if (e != cudaSuccess) return e;
+        if (per < 1) return cudaErrorInvalidConfiguration;
+        slots = sms * per;
+        std::lock_guard<std::mutex> lk(mu);
+        if (used < 256) cache[used++] = Slot{ fn, dev, slots };
+    }
+    const long g = std::min<long>(tiles, (long)slots);
+    *grid = (unsigned)std::max<long>(g, 1);
+    return cudaSuccess;
 }
 
 }  // namespace ppf

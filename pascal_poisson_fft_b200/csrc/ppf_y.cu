@@ -172,6 +172,85 @@ __global__ void __launch_bounds__(512) k_yinv(const cx<T>* __restrict__ in, long
     }
 }
 
+// Persistent, double-buffered complex y transform (forward, or inverse
+// with the zero-mode shift) for the compile-time shapes: each CTA walks the
+// (z, column block) tiles with a grid stride, and the next tile's columns
+// are copied into the second buffer with cp.async while the current tile
+// is transformed and stored, so the loads of one tile overlap the
+// butterflies of the previous one.
+template <typename T, bool INV, typename SH>
+__global__ void __launch_bounds__(SH::NT) k_y_c2c_pipe(const cx<T>* __restrict__ in, long in_pitch,
+                                                      cx<T>* __restrict__ out, long out_pitch, int ncols, int nz,
+                                                      const cx<T>* __restrict__ tw,
+                                                      const double* __restrict__ dc_shift,
+                                                      const int* __restrict__ skip)
+{
+    if (skip && *skip) return;
+    constexpr int N = SH::N, W = SH::W, NT = SH::NT;
+    constexpr int LGW = ct_log2y(W);
+    constexpr int EPT = (N * W) / NT;
+    static_assert(EPT * NT == N * W, "tile elements must divide over the threads");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<T>* cur = reinterpret_cast<cx<T>*>(smem_raw);
+    cx<T>* nxt = cur + N * W;
+    const int nblk = (ncols + W - 1) / W;
+    const long ntiles = (long)nblk * nz;
+    auto issue = [&](long t, cx<T>* b) {
+        const int z = (int)(t / nblk), col0 = (int)(t - (long)z * nblk) * W;
+        const cx<T>* inp = in + (long)z * N * in_pitch + col0;
+#pragma unroll
+        for (int i = 0; i < EPT; ++i) {
+            const int e = threadIdx.x + i * NT;
+            const int l = e & (W - 1), y = e >> LGW;
+            cx<T>* d = b + sidx_ct<T, W>(y, l);
+            if (col0 + l < ncols) cp_async_elem(d, inp + (long)y * in_pitch + l);
+            else *d = mk<T>((T)0, (T)0);
+        }
+        cp_async_commit();
+    };
+    long t = blockIdx.x;
+    if (t < ntiles) issue(t, cur);
+    for (; t < ntiles; t += gridDim.x) {
+        const long tn = t + gridDim.x;
+        if (tn < ntiles) issue(tn, nxt);
+        else cp_async_commit();
+        cp_async_wait<1>();  // this thread's copies of tile t have landed
+        const int z = (int)(t / nblk), col0 = (int)(t - (long)z * nblk) * W;
+        // the zero mode's z-average, removed from the (kx,ky) = (0,0) coefficient
+        // (element (0,0) is copied by thread 0)
+        if (INV && dc_shift && col0 == 0 && threadIdx.x == 0) cur[sidx_ct<T, W>(0, 0)].x -= (T)*dc_shift;
+        __syncthreads();
+        SH::template fft<T, INV>(cur, tw);
+        cx<T>* outp = out + (long)z * N * out_pitch + col0;
+#pragma unroll
+        for (int i = 0; i < EPT; ++i) {
+            const int e = threadIdx.x + i * NT;
+            const int l = e & (W - 1), k = e >> LGW;
+            if (col0 + l < ncols) outp[(long)k * out_pitch + l] = cur[sidx_ct<T, W>(k, l)];
+        }
+        __syncthreads();  // cur is refilled two tiles on
+        cx<T>* tmp = cur;
+        cur = nxt;
+        nxt = tmp;
+    }
+}
+
+template <typename T, bool INV, typename SH>
+cudaError_t launch_y_c2c_pipe(const cx<T>* in, long in_pitch, cx<T>* out, long out_pitch, int ncols, int nz,
+                              const cx<T>* tw, const double* dc_shift, const int* skip_flag, cudaStream_t st)
+{
+    auto kern = k_y_c2c_pipe<T, INV, SH>;
+    const size_t smem = 2 * (size_t)SH::N * SH::W * sizeof(cx<T>);
+    cudaError_t e = set_smem(kern, smem);
+    if (e != cudaSuccess) return e;
+    const long tiles = (long)((ncols + SH::W - 1) / SH::W) * nz;
+    unsigned grid = 0;
+    e = persistent_grid(kern, SH::NT, smem, tiles, &grid);
+    if (e != cudaSuccess) return e;
+    kern<<<grid, SH::NT, smem, st>>>(in, in_pitch, out, out_pitch, ncols, nz, tw, dc_shift, skip_flag);
+    return cudaGetLastError();
+}
+
 template <typename T>
 cudaError_t launch_yfwd(int kind, const cx<T>* in, long in_pitch, cx<T>* out, long out_pitch, int ncols,
                         const Geom& g, const FftSched& sch, const cx<T>* tw_ny, const cx<T>* tw_dct,
@@ -192,7 +271,11 @@ cudaError_t launch_yfwd(int kind, const cx<T>* in, long in_pitch, cx<T>* out, lo
                                               skip_flag);
             err = cudaGetLastError();
         };
-        if (kind == Y_C2C) go(k_yfwd<T, Y_C2C, SH>);
+        if (kind == Y_C2C) {
+            if constexpr (SH::CT) err = launch_y_c2c_pipe<T, false, SH>(in, in_pitch, out, out_pitch, ncols, g.nz,
+                                                                       tw_ny, nullptr, skip_flag, st);
+            else go(k_yfwd<T, Y_C2C, SH>);
+        }
         else if (kind == Y_CDCT) go(k_yfwd<T, Y_CDCT, SH>);
         else go(k_yfwd<T, Y_RPAIR, SH>);
     });
@@ -219,7 +302,11 @@ cudaError_t launch_yinv(int kind, const cx<T>* in, long in_pitch, cx<T>* out, lo
                                               dc_shift, skip_flag);
             err = cudaGetLastError();
         };
-        if (kind == Y_C2C) go(k_yinv<T, Y_C2C, SH>);
+        if (kind == Y_C2C) {
+            if constexpr (SH::CT) err = launch_y_c2c_pipe<T, true, SH>(in, in_pitch, out, out_pitch, ncols, g.nz,
+                                                                      tw_ny, dc_shift, skip_flag, st);
+            else go(k_yinv<T, Y_C2C, SH>);
+        }
         else if (kind == Y_CDCT) go(k_yinv<T, Y_CDCT, SH>);
         else go(k_yinv<T, Y_RPAIR, SH>);
     });
