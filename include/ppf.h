@@ -121,6 +121,17 @@ PPF_API int ppf_solve_host(ppf_plan *plan, const double *f_h, double *p_h,
                    const double *dmx1_h, const double *dmx2_h,
                    const double *dmx3_h, const double *dx3_h, void *stream);
 
+/* ppf_solve_host without the final synchronisation: the copies in, the
+ * solve and the copy out are enqueued on `stream` and the call returns.
+ * The host arrays must stay valid (and p_h unread) until the stream has
+ * finished; with page-locked host arrays the copies run asynchronously, so
+ * a caller that alternates two plans on two streams overlaps one solve's
+ * copy-out with the next solve's copy-in (they use separate copy engines).
+ * No reference counterpart (the reference solve is synchronous). */
+PPF_API int ppf_solve_host_async(ppf_plan *plan, const double *f_h, double *p_h,
+                   const double *dmx1_h, const double *dmx2_h,
+                   const double *dmx3_h, const double *dx3_h, void *stream);
+
 /* Number of refinement sweeps the last PPF_MIXED solve executed (device
  * early exit on sweep_tol), and ||du||/||u|| of its last sweep.  Reads two
  * device scalars (synchronises `stream`). */

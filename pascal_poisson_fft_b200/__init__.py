@@ -47,7 +47,7 @@ EXPORTED_SYMBOLS = (
     "ppf_fft_poisson_plan_cuda_create", "ppf_cuda_poisson_fft_initial", "ppf_cuda_poisson_fft_1d",
     "ppf_cuda_poisson_fft_clean", "ppf_cuda_poisson_fft_set_precision", "ppf_stage_timing",
     "ppf_stage_times", "ppf_solve_noalloc", "ppf_solve_adjoint", "ppf_batch_create", "ppf_batch_destroy",
-    "ppf_batch_solve", "ppf_batch_info",
+    "ppf_batch_solve", "ppf_batch_info", "ppf_solve_host_async",
 )
 PPF_BATCH_AUTOTUNE = 1
 STAGES = ("z-coefficients", "x-forward", "y-forward", "tdma-z", "y-inverse", "x-inverse",
@@ -88,6 +88,7 @@ def lib() -> ctypes.CDLL:
     L.ppf_plan_destroy.argtypes = [_vp]
     L.ppf_solve.argtypes = [_vp] + [_vp] * 6 + [_vp]
     L.ppf_solve_host.argtypes = [_vp] + [_vp] * 6 + [_vp]
+    L.ppf_solve_host_async.argtypes = [_vp] + [_vp] * 6 + [_vp]
     L.ppf_last_sweeps.argtypes = [_vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double), _vp]
     L.ppf_plan_workspace_bytes.argtypes = [_vp, ctypes.POINTER(ctypes.c_longlong)]
     L.ppf_tdma_many.argtypes = [_vp] * 4 + [ctypes.c_int, ctypes.c_int, _vp]
@@ -238,6 +239,19 @@ class Plan:
             self._h, f.ctypes.data, P.ctypes.data, *[a.ctypes.data for a in arrs],
             _stream_ptr(stream) if stream is not None else None))
         return P
+
+    def solve_host_async(self, f, P, dmx1, dmx2, dmx3, dx3, stream) -> None:
+        """Enqueue copy-in, solve and copy-out of host arrays on `stream`
+        (page-locked torch CPU tensors for asynchronous copies); returns at once."""
+        n3m, n2m, n1m = self.shape
+        cells, ghosted = n1m * n2m * n3m, (n1m + 2) * (n2m + 2) * (n3m + 2)
+        ptrs = []
+        for name, t, numel in (("f", f, cells), ("P", P, ghosted), ("dmx1", dmx1, n1m + 2),
+                               ("dmx2", dmx2, n2m + 2), ("dmx3", dmx3, n3m + 2), ("dx3", dx3, n3m + 2)):
+            if t.device.type != "cpu" or t.dtype.itemsize != 8 or not t.is_contiguous() or t.numel() != numel:
+                raise TypeError(f"{name} must be a contiguous float64 host tensor of {numel} elements")
+            ptrs.append(t.data_ptr())
+        _check("ppf_solve_host_async", lib().ppf_solve_host_async(self._h, *ptrs, _stream_ptr(stream)))
 
     def stage_timing(self, enable: bool) -> None:
         _check("ppf_stage_timing", lib().ppf_stage_timing(self._h, int(bool(enable))))

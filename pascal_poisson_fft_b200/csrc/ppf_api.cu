@@ -474,6 +474,46 @@ int adjoint_impl(ppf_plan* p, const double* g, double* df, const double* u, doub
     return PPF_OK;
 }
 
+// host arrays: copy in on `st`, solve, copy out; `sync` waits for the stream
+int host_impl(ppf_plan* plan, const double* f_h, double* p_h, const double* dmx1_h, const double* dmx2_h,
+              const double* dmx3_h, const double* dx3_h, cudaStream_t st, bool sync)
+{
+    g_err[0] = 0;
+    if (!plan) return fail(PPF_ERR_INVALID, "null plan");
+    if (!f_h || !p_h || !dmx1_h || !dmx2_h || !dmx3_h || !dx3_h) return fail(PPF_ERR_INVALID, "null array argument");
+    const Geom& g = plan->g;
+    const size_t nf = (size_t)g.nx * g.ny * g.nz, np = (size_t)(g.nx + 2) * (g.ny + 2) * (g.nz + 2);
+    const size_t nm = (size_t)(g.nx + 2) + (g.ny + 2) + 2 * (g.nz + 2);
+    if (!plan->f_dev) {
+        if (cudaMalloc((void**)&plan->f_dev, nf * sizeof(double)) != cudaSuccess ||
+            cudaMalloc((void**)&plan->p_dev, np * sizeof(double)) != cudaSuccess ||
+            cudaMalloc((void**)&plan->m_dev, nm * sizeof(double)) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(PPF_ERR_NOMEM, "cannot allocate device staging for host arrays");
+        }
+    }
+    double *fd = plan->f_dev, *pd = plan->p_dev;
+    double* d1 = plan->m_dev;
+    double* d2 = d1 + (g.nx + 2);
+    double* d3 = d2 + (g.ny + 2);
+    double* x3 = d3 + (g.nz + 2);
+    PPF_CK(cudaMemcpyAsync(fd, f_h, nf * sizeof(double), cudaMemcpyHostToDevice, st));
+    PPF_CK(cudaMemcpyAsync(d1, dmx1_h, (g.nx + 2) * sizeof(double), cudaMemcpyHostToDevice, st));
+    PPF_CK(cudaMemcpyAsync(d2, dmx2_h, (g.ny + 2) * sizeof(double), cudaMemcpyHostToDevice, st));
+    PPF_CK(cudaMemcpyAsync(d3, dmx3_h, (g.nz + 2) * sizeof(double), cudaMemcpyHostToDevice, st));
+    PPF_CK(cudaMemcpyAsync(x3, dx3_h, (g.nz + 2) * sizeof(double), cudaMemcpyHostToDevice, st));
+    int rc = solve_impl(plan, fd, pd, d1, d2, d3, x3, st);
+    if (rc == PPF_OK) {
+        cudaError_t e = cudaMemcpyAsync(p_h, pd, np * sizeof(double), cudaMemcpyDeviceToHost, st);
+        if (e != cudaSuccess) rc = cuda_fail(e, "copy out");
+    }
+    if (sync) {
+        cudaError_t e = cudaStreamSynchronize(st);
+        if (rc == PPF_OK && e != cudaSuccess) rc = cuda_fail(e, "synchronise");
+    }
+    return rc;
+}
+
 // one module-global plan for the reference-shaped API (p_poi, fft_3d_poisson.f90:43-59)
 std::mutex g_mod_mu;
 ppf_desc g_mod_desc{};
@@ -567,39 +607,13 @@ int ppf_solve_adjoint(ppf_plan* plan, const double* g_d, double* df_d, const dou
 int ppf_solve_host(ppf_plan* plan, const double* f_h, double* p_h, const double* dmx1_h, const double* dmx2_h,
                    const double* dmx3_h, const double* dx3_h, void* stream)
 {
-    g_err[0] = 0;
-    if (!plan) return fail(PPF_ERR_INVALID, "null plan");
-    if (!f_h || !p_h || !dmx1_h || !dmx2_h || !dmx3_h || !dx3_h) return fail(PPF_ERR_INVALID, "null array argument");
-    cudaStream_t st = (cudaStream_t)stream;
-    const Geom& g = plan->g;
-    const size_t nf = (size_t)g.nx * g.ny * g.nz, np = (size_t)(g.nx + 2) * (g.ny + 2) * (g.nz + 2);
-    const size_t nm = (size_t)(g.nx + 2) + (g.ny + 2) + 2 * (g.nz + 2);
-    if (!plan->f_dev) {
-        if (cudaMalloc((void**)&plan->f_dev, nf * sizeof(double)) != cudaSuccess ||
-            cudaMalloc((void**)&plan->p_dev, np * sizeof(double)) != cudaSuccess ||
-            cudaMalloc((void**)&plan->m_dev, nm * sizeof(double)) != cudaSuccess) {
-            cudaGetLastError();
-            return fail(PPF_ERR_NOMEM, "cannot allocate device staging for host arrays");
-        }
-    }
-    double *fd = plan->f_dev, *pd = plan->p_dev;
-    double* d1 = plan->m_dev;
-    double* d2 = d1 + (g.nx + 2);
-    double* d3 = d2 + (g.ny + 2);
-    double* x3 = d3 + (g.nz + 2);
-    PPF_CK(cudaMemcpyAsync(fd, f_h, nf * sizeof(double), cudaMemcpyHostToDevice, st));
-    PPF_CK(cudaMemcpyAsync(d1, dmx1_h, (g.nx + 2) * sizeof(double), cudaMemcpyHostToDevice, st));
-    PPF_CK(cudaMemcpyAsync(d2, dmx2_h, (g.ny + 2) * sizeof(double), cudaMemcpyHostToDevice, st));
-    PPF_CK(cudaMemcpyAsync(d3, dmx3_h, (g.nz + 2) * sizeof(double), cudaMemcpyHostToDevice, st));
-    PPF_CK(cudaMemcpyAsync(x3, dx3_h, (g.nz + 2) * sizeof(double), cudaMemcpyHostToDevice, st));
-    int rc = solve_impl(plan, fd, pd, d1, d2, d3, x3, st);
-    if (rc == PPF_OK) {
-        cudaError_t e = cudaMemcpyAsync(p_h, pd, np * sizeof(double), cudaMemcpyDeviceToHost, st);
-        if (e != cudaSuccess) rc = cuda_fail(e, "copy out");
-    }
-    cudaError_t e = cudaStreamSynchronize(st);
-    if (rc == PPF_OK && e != cudaSuccess) rc = cuda_fail(e, "synchronise");
-    return rc;
+    return host_impl(plan, f_h, p_h, dmx1_h, dmx2_h, dmx3_h, dx3_h, (cudaStream_t)stream, true);
+}
+
+int ppf_solve_host_async(ppf_plan* plan, const double* f_h, double* p_h, const double* dmx1_h, const double* dmx2_h,
+                         const double* dmx3_h, const double* dx3_h, void* stream)
+{
+    return host_impl(plan, f_h, p_h, dmx1_h, dmx2_h, dmx3_h, dx3_h, (cudaStream_t)stream, false);
 }
 
 int ppf_last_sweeps(ppf_plan* plan, int* sweeps, double* last_rel_update, void* stream)

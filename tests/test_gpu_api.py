@@ -38,6 +38,28 @@ def test_host_array_solve():
     assert rel_l2(P, oracle_solve(p)) < 1e-12
 
 
+def test_host_array_async_two_plans():
+    """ppf_solve_host_async on two plans and two streams, alternating over
+    different right-hand sides (page-locked host tensors)."""
+    import torch
+    rng = np.random.default_rng(34)
+    probs = [W.random_problem(rng, 40, 32, 24, (1, 1, 0), beta=1.5) for _ in range(4)]
+    p0 = probs[0]
+    m = p0.metrics
+    plans = [ppf.Plan(p0.n1m, p0.n2m, p0.n3m, p0.L1, p0.L2, *p0.pbc) for _ in range(2)]
+    streams = [torch.cuda.Stream(), torch.cuda.Stream()]
+    mh = [torch.as_tensor(np.ascontiguousarray(m[k])).pin_memory() for k in ("dmx1", "dmx2", "dmx3", "dx3")]
+    fh = [torch.as_tensor(q.f).pin_memory() for q in probs]
+    Ph = [torch.empty(p0.gshape if hasattr(p0, "gshape") else (p0.n3m + 2, p0.n2m + 2, p0.n1m + 2),
+                      dtype=torch.float64).pin_memory() for _ in probs]
+    for i in range(len(probs)):
+        plans[i % 2].solve_host_async(fh[i], Ph[i], *mh, stream=streams[i % 2])
+    torch.cuda.synchronize()
+    for q, P in zip(probs, Ph):
+        q.metrics = m
+        assert rel_l2(P.numpy(), oracle_solve(q)) < 1e-12
+
+
 def test_nan_rhs_is_reported():
     rng = np.random.default_rng(33)
     p = W.random_problem(rng, 16, 16, 16, (1, 1, 0))
