@@ -58,6 +58,17 @@ def dist_env():
     return ws, rank, lrank
 
 
+def max_over_ranks(value: float, ws: int, device=None) -> float:
+    """The job's time of a step: the slowest rank's (all ranks call this)."""
+    if ws == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 class ClockSampler:
     """nvidia-smi clocks / throttle reasons sampled every 200 ms while running."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -232,12 +243,7 @@ def run_ours(args, ws, rank, lrank):
             plan.solve(f, out, dmx1, dmx2, dmx3, dx3)
         e1.record(st)
         torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1) / k
-        if ws > 1:
-            tt = torch.tensor([ms], device=dev)
-            torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-            ms = float(tt.item())
-        return ms
+        return max_over_ranks(e0.elapsed_time(e1) / k, ws, dev)
 
     clocks = ClockSampler(dev.index if "CUDA_VISIBLE_DEVICES" not in os.environ else lrank)
     clocks.start()
@@ -300,11 +306,7 @@ def run_ours(args, ws, rank, lrank):
         ends = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
         e2e_steps(k2, e0, ends)
         torch.cuda.synchronize()
-        ms_e2e = max(e0.elapsed_time(ev) for ev in ends) / k2
-        if ws > 1:
-            tt = torch.tensor([ms_e2e], device=dev)
-            torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-            ms_e2e = float(tt.item())
+        ms_e2e = max_over_ranks(max(e0.elapsed_time(ev) for ev in ends) / k2, ws, dev)
         # the last step's result matches the device solve of the same input
         e2e_rel = float(torch.linalg.vector_norm(Ph[(k2 - 1) % 2].to(dev) - P64) / torch.linalg.vector_norm(P64))
         h2d = fh.nbytes + sum(a.nbytes for a in mh)
