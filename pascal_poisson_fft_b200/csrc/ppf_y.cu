@@ -235,6 +235,18 @@ __global__ void __launch_bounds__(SH::NT) k_y_c2c_pipe(const cx<T>* __restrict__
     }
 }
 
+// Tile shape of the pipelined y kernel.  FP64 tiles of 512-thread shapes
+// are halved (W/2 columns, 256 threads): two 32 KB buffers per CTA let three
+// CTAs share an SM, and 8 complex values per thread fit without spills.
+template <typename T, typename SH>
+struct PipeShape {
+    using type = SH;
+};
+template <int N, int W, int... RS>
+struct PipeShape<double, ShapeCT<N, W, 512, RS...>> {
+    using type = ShapeCT<N, W / 2, 256, RS...>;
+};
+
 template <typename T, bool INV, typename SH>
 cudaError_t launch_y_c2c_pipe(const cx<T>* in, long in_pitch, cx<T>* out, long out_pitch, int ncols, int nz,
                               const cx<T>* tw, const double* dc_shift, const int* skip_flag, cudaStream_t st)
@@ -272,8 +284,10 @@ cudaError_t launch_yfwd(int kind, const cx<T>* in, long in_pitch, cx<T>* out, lo
             err = cudaGetLastError();
         };
         if (kind == Y_C2C) {
-            if constexpr (SH::CT) err = launch_y_c2c_pipe<T, false, SH>(in, in_pitch, out, out_pitch, ncols, g.nz,
-                                                                       tw_ny, nullptr, skip_flag, st);
+            if constexpr (SH::CT)
+                err = launch_y_c2c_pipe<T, false, typename PipeShape<T, SH>::type>(in, in_pitch, out, out_pitch,
+                                                                                  ncols, g.nz, tw_ny, nullptr,
+                                                                                  skip_flag, st);
             else go(k_yfwd<T, Y_C2C, SH>);
         }
         else if (kind == Y_CDCT) go(k_yfwd<T, Y_CDCT, SH>);
@@ -303,8 +317,10 @@ cudaError_t launch_yinv(int kind, const cx<T>* in, long in_pitch, cx<T>* out, lo
             err = cudaGetLastError();
         };
         if (kind == Y_C2C) {
-            if constexpr (SH::CT) err = launch_y_c2c_pipe<T, true, SH>(in, in_pitch, out, out_pitch, ncols, g.nz,
-                                                                      tw_ny, dc_shift, skip_flag, st);
+            if constexpr (SH::CT)
+                err = launch_y_c2c_pipe<T, true, typename PipeShape<T, SH>::type>(in, in_pitch, out, out_pitch,
+                                                                                 ncols, g.nz, tw_ny, dc_shift,
+                                                                                 skip_flag, st);
             else go(k_yinv<T, Y_C2C, SH>);
         }
         else if (kind == Y_CDCT) go(k_yinv<T, Y_CDCT, SH>);
