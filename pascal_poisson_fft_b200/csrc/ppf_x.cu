@@ -131,17 +131,30 @@ __global__ void __launch_bounds__(512) k_xfwd(const double* __restrict__ f, Resi
 
     if (!DCT) {
         cx<T>* out = reinterpret_cast<cx<T>*>(out_);
-        const int Eo = (nc + 1) * W;
-        for (int e = threadIdx.x; e < Eo; e += NTH) {
-            const int l = e / (nc + 1), k = e - l * (nc + 1);
+        // R2C split, one pair (k, nc-k) per iteration from z_k and z_{nc-k}
+        const int NP = nc / 2 + 1;
+        for (int e = threadIdx.x; e < (NP << lgW); e += NTH) {
+            const int l = e / NP, k = e - l * NP;
             const long line = line0 + l;
             if (line >= nlines) continue;
-            const cx<T> zk = s[sidx<T>(k == nc ? 0 : k, l, W)];
-            const cx<T> zc = conj(s[sidx<T>(k == 0 ? 0 : nc - k, l, W)]);
-            const cx<T> Ev = (zk + zc) * (T)0.5;
-            const cx<T> D = zk - zc;
-            const cx<T> O = mk<T>(D.y * (T)0.5, -D.x * (T)0.5);
-            out[line * out_pitch + k] = Ev + cmul(ldg(tw_n + k), O);
+            const int kc = nc - k;
+            const cx<T> a = s[sidx<T>(k, l, W)];
+            const cx<T> b = s[sidx<T>(k == 0 ? 0 : kc, l, W)];
+            cx<T>* orow = out + line * out_pitch;
+            {
+                const cx<T> zc = conj(b);
+                const cx<T> Ev = (a + zc) * (T)0.5;
+                const cx<T> D = a - zc;
+                const cx<T> O = mk<T>(D.y * (T)0.5, -D.x * (T)0.5);
+                orow[k] = Ev + cmul(ldg(tw_n + k), O);
+            }
+            if (kc != k) {
+                const cx<T> zc = conj(a);
+                const cx<T> Ev = (b + zc) * (T)0.5;
+                const cx<T> D = b - zc;
+                const cx<T> O = mk<T>(D.y * (T)0.5, -D.x * (T)0.5);
+                orow[kc] = Ev + cmul(ldg(tw_n + kc), O);
+            }
         }
     } else {
         // X_k = 2 Re(e^{-i pi k/(2n)} V_k), V_{n-k} = conj(V_k)
@@ -200,6 +213,36 @@ __global__ void __launch_bounds__(512) k_xinv(const void* __restrict__ in_, long
                         (unsigned)((nx + 2) * sizeof(double)));
     }
 
+    if constexpr (!DCT) {
+        // C2R split, one pair (k, nc-k) per iteration: Z_k from (X_k, conj X_{nc-k}),
+        // Z_{nc-k} from (X_{nc-k}, conj X_k)
+        const int NP = nc / 2 + 1;
+        for (int e = threadIdx.x; e < (NP << lgW); e += NTH) {
+            const int l = e / NP, k = e - l * NP;
+            const int kc = nc - k;
+            const long line = line0 + l;
+            cx<T> Zk = mk<T>((T)0, (T)0), Zc = Zk;
+            if (line < nlines) {
+                const cx<T>* row = reinterpret_cast<const cx<T>*>(in_) + line * in_pitch;
+                cx<T> xa = row[k], xb = row[kc];
+                if (k == 0) { xa.y = (T)0; xb.y = (T)0; }
+                {
+                    const cx<T> c = conj(xb);
+                    const cx<T> Ev = xa + c, D = xa - c;
+                    const cx<T> O = cmul(D, conj(ldg(tw_n + k)));
+                    Zk = mk<T>(Ev.x - O.y, Ev.y + O.x);
+                }
+                {
+                    const cx<T> c = conj(xa);
+                    const cx<T> Ev = xb + c, D = xb - c;
+                    const cx<T> O = cmul(D, conj(ldg(tw_n + kc)));
+                    Zc = mk<T>(Ev.x - O.y, Ev.y + O.x);
+                }
+            }
+            s[sidx<T>(k, l, W)] = Zk;
+            if (k != 0 && kc != k) s[sidx<T>(kc, l, W)] = Zc;
+        }
+    } else
     for (int e = threadIdx.x; e < E; e += NTH) {
         const int l = e / nc, k = e - l * nc;
         const long line = line0 + l;
@@ -256,33 +299,67 @@ __global__ void __launch_bounds__(512) k_xinv(const void* __restrict__ in_, long
     double acc_du = 0.0, acc_u = 0.0, acc_s = 0.0;
     const double mprev = (ACC && mean_prev) ? *mean_prev : 0.0;
     const int Eo = nx << lgW;
-    for (int e = threadIdx.x; e < Eo; e += NTH) {
-        const int l = e / nx, i = e - l * nx;
-        const long line = line0 + l;
-        if (line >= nlines) continue;
-        int n = i;
-        // inverse Makhoul order (cuda_Poisson_DCT_b_post, :1013-1033)
-        if (DCT) n = (i & 1) ? (nc + ((nx - 1 - i) >> 1)) : (i >> 1);
-        const cx<T> zv = s[sidx<T>(n >> 1, l, W)];
-        const double x = (double)((n & 1) ? zv.y : zv.x);
-        const long o = line_base[l] + i;
-        // refinement: u <- u + du - mean(u), the FP64 mean of the previous
-        // iterate (the residual cannot see constants, so the gauge is kept here)
-        const double un = ACC ? (P[o] - mprev) + x : x;
-        P[o] = un;
-        if (GHOST) {
-            // stencil ghosts for the next residual (the reference's ghost
-            // update overwrites them after the last sweep)
-            if (i == 0) P[o + (g.px ? nx : -1)] = un;
-            if (i == nx - 1) P[o + (g.px ? -nx : 1)] = un;
-            const long gy = line_gy[l], gz = line_gz[l];
-            if (gy) P[o + gy] = un;
-            if (gz) P[o + gz] = un;
+    if constexpr (!DCT) {
+        // periodic x: outputs x_2n, x_2n+1 are Re, Im of z_n -- two per iteration
+        for (int e = threadIdx.x; e < E; e += NTH) {
+            const int l = e / nc, n = e - l * nc;
+            if (line0 + l >= nlines) continue;
+            const cx<T> zv = s[sidx<T>(n, l, W)];
+            const double x0 = (double)zv.x, x1 = (double)zv.y;
+            const long o = line_base[l] + 2 * n;
+            // refinement: u <- u + du - mean(u), the FP64 mean of the previous
+            // iterate (the residual cannot see constants, so the gauge is kept here)
+            double u0 = x0, u1 = x1;
+            if (ACC) {
+                u0 = (P[o] - mprev) + x0;
+                u1 = (P[o + 1] - mprev) + x1;
+            }
+            P[o] = u0;
+            P[o + 1] = u1;
+            if (GHOST) {
+                // stencil ghosts for the next residual (the reference's ghost
+                // update overwrites them after the last sweep)
+                if (n == 0) P[o + (g.px ? nx : -1)] = u0;
+                if (n == nc - 1) P[o + 1 + (g.px ? -nx : 1)] = u1;
+                const long gy = line_gy[l], gz = line_gz[l];
+                if (gy) { P[o + gy] = u0; P[o + 1 + gy] = u1; }
+                if (gz) { P[o + gz] = u0; P[o + 1 + gz] = u1; }
+            }
+            if (partials) {
+                acc_du += x0 * x0 + x1 * x1;
+                acc_u += u0 * u0 + u1 * u1;
+                acc_s += u0 + u1;
+            }
         }
-        if (partials) {
-            acc_du += x * x;
-            acc_u += un * un;
-            acc_s += un;
+    } else {
+        for (int e = threadIdx.x; e < Eo; e += NTH) {
+            const int l = e / nx, i = e - l * nx;
+            const long line = line0 + l;
+            if (line >= nlines) continue;
+            int n = i;
+            // inverse Makhoul order (cuda_Poisson_DCT_b_post, :1013-1033)
+            if (DCT) n = (i & 1) ? (nc + ((nx - 1 - i) >> 1)) : (i >> 1);
+            const cx<T> zv = s[sidx<T>(n >> 1, l, W)];
+            const double x = (double)((n & 1) ? zv.y : zv.x);
+            const long o = line_base[l] + i;
+            // refinement: u <- u + du - mean(u), the FP64 mean of the previous
+            // iterate (the residual cannot see constants, so the gauge is kept here)
+            const double un = ACC ? (P[o] - mprev) + x : x;
+            P[o] = un;
+            if (GHOST) {
+                // stencil ghosts for the next residual (the reference's ghost
+                // update overwrites them after the last sweep)
+                if (i == 0) P[o + (g.px ? nx : -1)] = un;
+                if (i == nx - 1) P[o + (g.px ? -nx : 1)] = un;
+                const long gy = line_gy[l], gz = line_gz[l];
+                if (gy) P[o + gy] = un;
+                if (gz) P[o + gz] = un;
+            }
+            if (partials) {
+                acc_du += x * x;
+                acc_u += un * un;
+                acc_s += un;
+            }
         }
     }
     if (partials) {
