@@ -291,7 +291,7 @@ int plan_init(ppf_plan* p, const ppf_desc* d)
     PPF_CK(cudaMalloc(&p->flags, sizeof(int) * 4));
     PPF_CK(cudaMemset(p->scal, 0, sizeof(double) * 8));
     PPF_CK(cudaMemset(p->flags, 0, sizeof(int) * 4));
-    p->ckpt_doubles = tdma_z_ckpt_doubles(nz, p->b_pitch * (long)p->my, p->g.pz);
+    p->ckpt_doubles = tdma_z_ckpt_doubles(nz, p->b_pitch * (long)p->my, p->g.pz, p->elem == 4);
     if (p->elem == 4) {
         PPF_CK(cudaStreamCreateWithFlags(&p->aux, cudaStreamNonBlocking));
         PPF_CK(cudaEventCreateWithFlags(&p->ev_fork, cudaEventDisableTiming));
@@ -366,6 +366,7 @@ int run_pass(ppf_plan* p, const double* f, double* P, bool resid, bool accumulat
     z.dc_shift = p->scal + 4;
     z.cyclic = p->g.pz;
     z.ckpt = p->ckpt;
+    z.ckpt_f = (sizeof(T) == 4) ? tdma_z_ckpt_f32(p->ckpt, z.nz, z.plane, z.cyclic) : nullptr;
     const ZStreams zs{ st, p->aux, p->ev_fork, p->ev_join };
     e = p->cplx ? launch_tdma_z<T, true>(p->B, z, skip, p->flags + 2, zs)
                 : launch_tdma_z<T, false>(p->B, z, skip, p->flags + 2, zs);
@@ -848,7 +849,7 @@ extern "C" int ppf_solve_noalloc(const ppf_desc* desc, const double* f_d, double
     const size_t oSc = off; off = na_align(off + sizeof(double) * 8);
     const size_t oFl = off; off = na_align(off + sizeof(int) * 4);
     const size_t oTw = off; off = na_align(off + sizeof(double) * tw_doubles);
-    const size_t oCk = off; off = na_align(off + sizeof(double) * tdma_z_ckpt_doubles(nz, p.b_pitch * (long)p.my, p.g.pz));
+    const size_t oCk = off; off = na_align(off + sizeof(double) * tdma_z_ckpt_doubles(nz, p.b_pitch * (long)p.my, p.g.pz, false));
     if (off > (size_t)PPF_NOALLOC_SCRATCH_BYTES)
         return fail(PPF_ERR_UNSUPPORTED,
                     "grid %dx%dx%d needs %zu bytes of work memory; ppf_solve_noalloc holds %zu (use ppf_plan_create)",

@@ -69,11 +69,14 @@ struct ZSys {
     const double* dzmax2; // device scalar: max_k dx3_k^2 (written by the z-coefficient kernel)
     double* dc_shift;     // device scalar: z-average of the (0,0) solution (subtracted by the y inverse)
     int cyclic;           // periodic z: the reference's cyclic Thomas sequence
-    double* ckpt;         // Thomas checkpoints, tdma_z_ckpt_doubles(nz, plane, cyclic) doubles
+    double* ckpt;         // Thomas checkpoints, tdma_z_ckpt_doubles(nz, plane, cyclic, fp32) doubles
+    float* ckpt_f;        // FP32 checkpoints of the FP32 bulk kernel (tdma_z_ckpt_f32), or null
 };
 
-// doubles of checkpoint memory the z solve needs
-long tdma_z_ckpt_doubles(int nz, long plane, int cyclic);
+// doubles of checkpoint memory the z solve needs (fp32: FP32 spectral storage)
+long tdma_z_ckpt_doubles(int nz, long plane, int cyclic, bool fp32);
+// start of the FP32 checkpoint region inside a checkpoint buffer of FP32 storage
+float* tdma_z_ckpt_f32(double* ckpt, int nz, long plane, int cyclic);
 
 // streams of the z solve: the FP32 bulk runs on st; the FP64 low-|k|
 // systems run on aux (forked from and joined back to st through the two

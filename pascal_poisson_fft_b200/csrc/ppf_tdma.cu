@@ -14,7 +14,7 @@
 //
 // The reference writes c' and d' of every row back to global memory and
 // reads them again in the back substitution.  Here the forward sweep keeps
-// only a checkpoint (c', d') every CH rows in shared memory; the backward
+// only a checkpoint (c', d') every CH rows in global memory; the backward
 // sweep re-reads the CH right-hand sides of a chunk, recomputes its c', d'
 // from the checkpoint (the same operations, so the same bits) and
 // substitutes.  Per row the field is read twice and written once.
@@ -373,15 +373,128 @@ __global__ void __launch_bounds__(TPB) k_thomas_z(void* __restrict__ data_, ZSys
     if (bad && err) atomicOr(err, 1);
 }
 
-long tdma_z_ckpt_doubles(int nz, long plane, int cyclic)
+long tdma_z_ckpt_doubles(int nz, long plane, int cyclic, bool fp32)
 {
     const int m = cyclic ? nz - 1 : nz;
     const int ch = Exact::CH < Fast::CH ? Exact::CH : Fast::CH;   // the finer chunking of the two paths
     const long nch = (m + ch - 1) / ch;
-    return nch * (cyclic ? 4 : 3) * plane;
+    const long dbl = nch * (cyclic ? 4 : 3) * plane;
+    // FP32 storage: FP32 checkpoints of the bulk kernel follow the FP64 ones
+    return fp32 ? dbl + (dbl + 1) / 2 : dbl;
+}
+
+float* tdma_z_ckpt_f32(double* ckpt, int nz, long plane, int cyclic)
+{
+    return reinterpret_cast<float*>(ckpt + tdma_z_ckpt_doubles(nz, plane, cyclic, false));
 }
 
 namespace {
+// FP32 bulk of the mixed-precision z solve (systems with lam dz_max^2 >=
+// lowk, non-periodic z).  The same Thomas sweep as thomas_poisson<Fast>,
+// with the level coefficients (am, ap, -am-ap) staged once per CTA in shared
+// memory (b = -am-ap - lam, a single rounding more than the FP64 order,
+// which the refinement absorbs), FP32 checkpoints in their own region, and
+// the next chunk's rows loaded while the current chunk is eliminated.
+template <bool CPLX>
+__global__ void __launch_bounds__(TPB) k_thomas_fast(void* __restrict__ data_, ZSys z, const int* __restrict__ skip,
+                                                     int* __restrict__ err)
+{
+    if (skip && *skip) return;
+    extern __shared__ float4 zlev[];
+    for (int k = threadIdx.x; k < z.nz; k += TPB) {
+        const double am = z.am[k], ap = z.ap[k];
+        zlev[k] = make_float4((float)am, (float)ap, (float)(-am - ap), 0.f);
+    }
+    __syncthreads();
+    using E = typename Elem<float, CPLX>::type;
+    const long sys = (long)blockIdx.x * TPB + threadIdx.x;
+    const int kx = (int)(sys % z.pitch), ky = (int)(sys / z.pitch);
+    if (kx >= z.mx || ky >= z.my) return;
+    const double lam = z.lamx[kx] + z.lamy[ky];
+    if (lam * __ldg(z.dzmax2) < z.lowk) return;  // solved in FP64 (includes the pinned zero mode)
+    const float lamf = (float)lam, sc = (float)z.scale;
+    const int nz = z.nz;
+    const long plane = z.plane;
+    constexpr int C = Fast::CH;
+    const int nch = (nz + C - 1) / C;
+    E* col = reinterpret_cast<E*>(data_) + sys;
+    float* ck = z.ckpt_f + sys;
+    float nr[C], ni[C];
+    auto load = [&](int z0) {
+#pragma unroll
+        for (int q = 0; q < C; ++q) {
+            nr[q] = 0.f;
+            ni[q] = 0.f;
+            if (z0 + q < nz) ld_cv<float, float>(col + (long)(z0 + q) * plane, nr[q], ni[q]);
+        }
+    };
+    load(0);
+    float cp = 0.f, dr = 0.f, di = 0.f;
+    for (int ch = 0; ch < nch; ++ch) {
+        float vr[C], vi[C];
+#pragma unroll
+        for (int q = 0; q < C; ++q) { vr[q] = nr[q]; vi[q] = ni[q]; }
+        if (ch + 1 < nch) load((ch + 1) * C);
+        const int z0 = ch * C;
+#pragma unroll
+        for (int q = 0; q < C; ++q) {
+            const int zr = z0 + q;
+            if (zr < nz) {
+                const float4 lv = zlev[zr];
+                fwd_row<Fast, CPLX>(zr == 0, lv.x, lv.z - lamf, lv.y, vr[q], vi[q], cp, dr, di);
+            }
+        }
+        float* c3 = ck + (long)(3 * ch) * plane;
+        c3[0] = cp;
+        c3[plane] = dr;
+        if (CPLX) c3[2 * plane] = di;
+    }
+    float xr = 0.f, xi = 0.f;
+    bool bad = false;
+    load((nch - 1) * C);
+    for (int ch = nch - 1; ch >= 0; --ch) {
+        float vr[C], vi[C], c_[C];
+#pragma unroll
+        for (int q = 0; q < C; ++q) { vr[q] = nr[q]; vi[q] = ni[q]; }
+        float pcp = 0.f, pdr = 0.f, pdi = 0.f;
+        if (ch > 0) {
+            const float* c3 = ck + (long)(3 * (ch - 1)) * plane;
+            pcp = c3[0];
+            pdr = c3[plane];
+            if (CPLX) pdi = c3[2 * plane];
+            load((ch - 1) * C);
+        }
+        const int z0 = ch * C;
+#pragma unroll
+        for (int q = 0; q < C; ++q) {
+            const int zr = z0 + q;
+            if (zr < nz) {
+                const float4 lv = zlev[zr];
+                fwd_row<Fast, CPLX>(zr == 0, lv.x, lv.z - lamf, lv.y, vr[q], vi[q], pcp, pdr, pdi);
+            }
+            c_[q] = pcp; vr[q] = pdr; vi[q] = pdi;
+        }
+#pragma unroll
+        for (int q = C - 1; q >= 0; --q) {
+            const int zr = z0 + q;
+            if (zr < nz) {
+                if (zr == nz - 1) {
+                    xr = vr[q];
+                    xi = vi[q];
+                } else {
+                    xr = vr[q] - c_[q] * xr;
+                    if (CPLX) xi = vi[q] - c_[q] * xi;
+                }
+                if (!isfinite(xr) || !isfinite(xi)) bad = true;
+                E* o = col + (long)zr * plane;
+                if constexpr (CPLX) *o = mk<float>(xr * sc, xi * sc);
+                else *o = xr * sc;
+            }
+        }
+    }
+    if (bad && err) atomicOr(err, 1);
+}
+
 template <bool CPLX, bool CYC>
 cudaError_t launch_z(double*, const ZSys& z, void* data, const int* skip, int* err, const ZStreams& zs)
 {
@@ -404,7 +517,10 @@ cudaError_t launch_z(float*, const ZSys& z, void* data, const int* skip, int* er
         lo = zs.aux;
     }
     k_thomas_z<float, Exact, CPLX, 2, CYC><<<grid, TPB, 0, lo>>>(data, z, skip, err);
-    k_thomas_z<float, Fast, CPLX, 1, CYC><<<grid, TPB, 0, zs.st>>>(data, z, skip, err);
+    if (CYC || !z.ckpt_f)
+        k_thomas_z<float, Fast, CPLX, 1, CYC><<<grid, TPB, 0, zs.st>>>(data, z, skip, err);
+    else
+        k_thomas_fast<CPLX><<<grid, TPB, sizeof(float4) * z.nz, zs.st>>>(data, z, skip, err);
     if (zs.aux) {
         cudaError_t e = cudaEventRecord(zs.join, zs.aux);
         if (e == cudaSuccess) e = cudaStreamWaitEvent(zs.st, zs.join, 0);
