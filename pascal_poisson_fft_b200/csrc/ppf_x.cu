@@ -385,6 +385,152 @@ __global__ void __launch_bounds__(512) k_xinv(const void* __restrict__ in_, long
 }
 
 // --------------------------------------------------------------------------
+// x inverse of FP32 spectra, periodic x, compile-time shapes: persistent
+// CTAs walk tiles of W lines; the next tile's half-spectrum rows are copied
+// with cp.async into the second of two raw buffers ([k][line], nc+1 rows)
+// while the current tile is split in place (C2R, pairs (k, nc-k)),
+// transformed and written out -- the output semantics of
+// k_xinv<T, false, ACC, GHOST>.  (FP64 tiles take the non-pipelined kernel:
+// two 66 KB buffers at 128 registers leave too few resident CTAs.)
+// --------------------------------------------------------------------------
+template <typename T, bool ACC, bool GHOST, typename SH>
+__global__ void __launch_bounds__(SH::NT) k_xinv_pipe(const cx<T>* __restrict__ in, long in_pitch,
+                                                     double* __restrict__ P, Geom g, double* __restrict__ partials,
+                                                     const double* __restrict__ mean_prev,
+                                                     const cx<T>* __restrict__ tw_half,
+                                                     const cx<T>* __restrict__ tw_n, const int* __restrict__ skip)
+{
+    if (skip && *skip) return;
+    constexpr int NC = SH::N, W = SH::W, NT = SH::NT;
+    constexpr int LGW = ct_log2(W);
+    constexpr int NR = NC + 1;
+    constexpr int ER = NR * W;
+    constexpr int NX = 2 * NC;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<T>* cur = reinterpret_cast<cx<T>*>(smem_raw);
+    cx<T>* nxt = cur + ER;
+    __shared__ long line_base[W], line_gy[W], line_gz[W];
+    const long nlines = (long)g.ny * g.nz;
+    const long ntiles = (nlines + W - 1) / W;
+    const bool pf = (reinterpret_cast<size_t>(P) & 15) == 0;
+    auto issue = [&](long t, cx<T>* b) {
+        const long line0 = t * W;
+        for (int e = threadIdx.x; e < ER; e += NT) {
+            const int l = e / NR, k = e - l * NR;
+            cx<T>* d = b + sidx_ct<T, W>(k, l);
+            if (line0 + l < nlines) cp_async_elem(d, in + (line0 + l) * in_pitch + k);
+            else *d = mk<T>((T)0, (T)0);
+        }
+        cp_async_commit();
+    };
+    double acc_du = 0.0, acc_u = 0.0, acc_s = 0.0;
+    const double mprev = (ACC && mean_prev) ? *mean_prev : 0.0;
+    long t = blockIdx.x;
+    if (t < ntiles) issue(t, cur);
+    for (; t < ntiles; t += gridDim.x) {
+        const long line0 = t * W;
+        const long tn = t + gridDim.x;
+        if (tn < ntiles) issue(tn, nxt);
+        else cp_async_commit();
+        // this tile's P rows into L2 ahead of the read-modify-write
+        if (ACC && pf && threadIdx.x < W && line0 + threadIdx.x < nlines) {
+            const long line = line0 + threadIdx.x;
+            prefetch_l2(P + (line % g.ny + 1) * g.pstride_y + (line / g.ny + 1) * g.pstride_z,
+                        (unsigned)((NX + 2) * sizeof(double)));
+        }
+        for (int l = threadIdx.x; l < W; l += NT) {
+            const long line = line0 + l;
+            const long j = line % g.ny, k = line / g.ny;
+            line_base[l] = 1 + (j + 1) * g.pstride_y + (k + 1) * g.pstride_z;
+            if (GHOST) {
+                long gy = 0;
+                if (j == 0) gy = g.py ? (long)g.ny * g.pstride_y : -g.pstride_y;
+                else if (j == g.ny - 1) gy = g.py ? -(long)g.ny * g.pstride_y : g.pstride_y;
+                long gz = 0;
+                if (k == 0) gz = -g.pstride_z;
+                else if (k == g.nz - 1) gz = g.pstride_z;
+                line_gy[l] = gy;
+                line_gz[l] = gz;
+            }
+        }
+        cp_async_wait<1>();  // this thread's copies of tile t have landed
+        __syncthreads();
+        // C2R split in place, one pair (k, nc-k) per iteration
+        for (int e = threadIdx.x; e < (NC / 2 + 1) * W; e += NT) {
+            const int l = e & (W - 1), k = e >> LGW;
+            const int kc = NC - k;
+            cx<T> xk = cur[sidx_ct<T, W>(k, l)];
+            cx<T> xc = cur[sidx_ct<T, W>(kc, l)];
+            if (k == 0) { xk.y = (T)0; xc.y = (T)0; }
+            const cx<T> wk = ldg(tw_n + k), wc = ldg(tw_n + kc);
+            {
+                const cx<T> a = xk, b = conj(xc);
+                const cx<T> Ev = a + b, D = a - b;
+                const cx<T> O = cmul(D, conj(wk));
+                cur[sidx_ct<T, W>(k, l)] = mk<T>(Ev.x - O.y, Ev.y + O.x);
+            }
+            if (k != 0 && kc != k) {
+                const cx<T> a = xc, b = conj(xk);
+                const cx<T> Ev = a + b, D = a - b;
+                const cx<T> O = cmul(D, conj(wc));
+                cur[sidx_ct<T, W>(kc, l)] = mk<T>(Ev.x - O.y, Ev.y + O.x);
+            }
+        }
+        __syncthreads();
+        SH::template fft<T, true>(cur, tw_half);
+        for (int e = threadIdx.x; e < NC * W; e += NT) {
+            const int l = e / NC, n = e - l * NC;
+            if (line0 + l >= nlines) continue;
+            const cx<T> zv = cur[sidx_ct<T, W>(n, l)];
+            const double x0 = (double)zv.x, x1 = (double)zv.y;
+            const long o = line_base[l] + 2 * n;
+            double u0 = x0, u1 = x1;
+            if (ACC) {
+                u0 = (P[o] - mprev) + x0;
+                u1 = (P[o + 1] - mprev) + x1;
+            }
+            P[o] = u0;
+            P[o + 1] = u1;
+            if (GHOST) {
+                if (n == 0) P[o + (g.px ? NX : -1)] = u0;
+                if (n == NC - 1) P[o + 1 + (g.px ? -NX : 1)] = u1;
+                const long gy = line_gy[l], gz = line_gz[l];
+                if (gy) { P[o + gy] = u0; P[o + 1 + gy] = u1; }
+                if (gz) { P[o + gz] = u0; P[o + 1 + gz] = u1; }
+            }
+            if (partials) {
+                acc_du += x0 * x0 + x1 * x1;
+                acc_u += u0 * u0 + u1 * u1;
+                acc_s += u0 + u1;
+            }
+        }
+        __syncthreads();  // cur and the line tables are refilled
+        cx<T>* tmp = cur;
+        cur = nxt;
+        nxt = tmp;
+    }
+    if (partials) {
+        __shared__ double red[3][32];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            acc_du += __shfl_down_sync(0xffffffffu, acc_du, off);
+            acc_u += __shfl_down_sync(0xffffffffu, acc_u, off);
+            acc_s += __shfl_down_sync(0xffffffffu, acc_s, off);
+        }
+        const int w = threadIdx.x >> 5;
+        if ((threadIdx.x & 31) == 0) { red[0][w] = acc_du; red[1][w] = acc_u; red[2][w] = acc_s; }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double a = 0, b = 0, c = 0;
+            for (int q = 0; q < NT / 32; ++q) { a += red[0][q]; b += red[1][q]; c += red[2][q]; }
+            partials[3 * blockIdx.x + 0] = a;
+            partials[3 * blockIdx.x + 1] = b;
+            partials[3 * blockIdx.x + 2] = c;
+        }
+    }
+}
+
+// --------------------------------------------------------------------------
 // launchers
 // --------------------------------------------------------------------------
 template <typename T>
@@ -444,6 +590,25 @@ cudaError_t launch_xinv(bool dct, const void* in, long in_pitch, double* P, cons
                                               tw_n, tw_dct, skip_flag);
             err = cudaGetLastError();
         };
+        if constexpr (SH::CT && sizeof(T) == 4) {
+            if (!dct) {  // pipelined FP32 tiles
+                auto pipe = [&](auto kern) {
+                    const size_t psmem = 2 * (size_t)(SH::N + 1) * SH::W * sizeof(cx<T>);
+                    err = set_smem(kern, psmem);
+                    unsigned pgrid = 0;
+                    if (err == cudaSuccess) err = persistent_grid(kern, SH::NT, psmem, (long)grid.x, &pgrid);
+                    if (err != cudaSuccess) return;
+                    if (blocks_used) *blocks_used = pgrid;
+                    kern<<<pgrid, SH::NT, psmem, st>>>(reinterpret_cast<const cx<T>*>(in), in_pitch, P, g, partials,
+                                                      mean_prev, tw_half, tw_n, skip_flag);
+                    err = cudaGetLastError();
+                };
+                if (!stencil_ghosts) pipe(k_xinv_pipe<T, false, false, SH>);
+                else if (accumulate) pipe(k_xinv_pipe<T, true, true, SH>);
+                else pipe(k_xinv_pipe<T, false, true, SH>);
+                return;
+            }
+        }
         if (stencil_ghosts) {
             if (dct) {
                 if (accumulate) go(k_xinv<T, true, true, true, SH>);
