@@ -168,6 +168,52 @@ PPF_API int ppf_tdma_many(const double *a, const double *b, const double *c, dou
 PPF_API int ppf_tdma_cycl_many(const double *a, const double *b, const double *c, double *d,
                        int n_sys, int n_row, void *stream);
 
+/* Systems whose rows are split over ranks (z slabs), PaScaL_TDMA_many_solve_cuda
+ * at nprocs > 1 (pascal_tdma_cuda.f90:243-266).  Step 1,
+ * ppf_tdma_many_modified: the modified Thomas algorithm on this rank's
+ * n_row (>= 3) rows (pascal_tdma_cuda.f90:332-473); a, c, d are overwritten
+ * with the modified coefficients, b is read only, and the rank's two reduced
+ * rows (b = 1) go to a_rd, c_rd, d_rd, element (sys, r) at [r * n_sys + sys],
+ * r = 0 for the first local row, 1 for the last.  The caller gathers the
+ * reduced rows of all ranks per system (2 * nranks rows, rank-major) and
+ * solves them (ppf_tdma_many with b = 1), then step 2,
+ * ppf_tdma_many_update (pascal_tdma_cuda.f90:483-520), finishes the local
+ * rows from the reduced solution x_rd (same layout as d_rd).
+ * pascal_poisson_fft_b200.dist drives the exchange with torch.distributed. */
+PPF_API int ppf_tdma_many_modified(double *a, const double *b, double *c, double *d,
+                           double *a_rd, double *c_rd, double *d_rd,
+                           int n_sys, int n_row, void *stream);
+PPF_API int ppf_tdma_many_update(const double *a, const double *c, double *d, const double *x_rd,
+                         int n_sys, int n_row, void *stream);
+
+/* z-slab (multi-rank) FP64 solve, the reference's np3 > 1 decomposition of
+ * cuda_Poisson_FFT_1D (fft_3d_poisson.f90:353-626): the plan describes this
+ * rank's slab (n3m = its z rows); pascal_poisson_fft_b200.dist.SlabPoisson
+ * drives the steps and the exchanges between ranks.
+ *   ppf_slab_systems:   doubles per z row of the spectrum (= systems: real and
+ *                       imaginary parts are separate systems).
+ *   ppf_slab_forward:   x and y forward transforms of f into spec (n3m rows).
+ *   ppf_slab_coefficients: a, b, c of this rank's rows z0 .. z0+n3m-1 of the
+ *                       global z operator (global dx3_g, dmx3_g of n3m_g+2
+ *                       values), the pin at the global first row, and the
+ *                       normalisation applied to spec; then the multi-rank
+ *                       TDMA (ppf_tdma_many_modified / _update) solves spec.
+ *   ppf_slab_inverse:   inverse transforms of spec into the interior of P.
+ *   ppf_slab_sum:       deterministic interior sum of P into *sum_d (device).
+ *   ppf_slab_shift:     P -= *shift_d on the interior (the global mean).
+ *   ppf_slab_ghosts:    ghost update in the reference's order with z walls
+ *                       only where flagged (the global ends); the ghost planes
+ *                       between slabs must hold the neighbours' planes first. */
+PPF_API int ppf_slab_systems(const ppf_plan *plan, int *n_sys);
+PPF_API int ppf_slab_forward(ppf_plan *plan, const double *f_d, double *spec_d, void *stream);
+PPF_API int ppf_slab_coefficients(ppf_plan *plan, double *a_d, double *b_d, double *c_d, double *spec_d,
+                          const double *dx3_g, const double *dmx3_g, int z0, int n3m_g, void *stream);
+PPF_API int ppf_slab_inverse(ppf_plan *plan, const double *spec_d, double *p_d, void *stream);
+PPF_API int ppf_slab_sum(ppf_plan *plan, const double *p_d, double *sum_d, void *stream);
+PPF_API int ppf_slab_shift(ppf_plan *plan, double *p_d, const double *shift_d, void *stream);
+PPF_API int ppf_slab_ghosts(ppf_plan *plan, double *p_d, const double *dmx1_d, const double *dmx2_d,
+                    const double *dmx3_d, int z_lo_wall, int z_hi_wall, void *stream);
+
 /* Allocation-free FP64 solve, for callers that cannot allocate device
  * memory at solve time: a flow solver that reserved its whole device memory
  * budget at start-up, or an application whose memory is owned by another

@@ -211,3 +211,38 @@ def poisson_adjoint(g, L1, L2, pbc, dmx1, dmx2, dmx3, dx3, u=None):
     ddmx3[1:n3m + 1] += -dam * am / dmx3[1:n3m + 1]
     ddmx3[2:n3m + 2] += -dap * ap / dmx3[2:n3m + 2]
     return df, ddx3, ddmx3
+
+
+def tdma_modified(a, b, c, d):
+    """This rank's part of PaScaL_TDMA_many_solve at nprocs > 1
+    (01_Fortran/PaScaL_TDMA/src/pascal_tdma.f90:522-566): the modified Thomas
+    sweep on arrays of shape (n_row, n_sys), in place on a, c, d; returns the
+    reduced rows (a_rd, c_rd, d_rd), each (2, n_sys) (b_rd = 1)."""
+    n = d.shape[0]
+    for j in (0, 1):
+        a[j] /= b[j]
+        d[j] /= b[j]
+        c[j] /= b[j]
+    for j in range(2, n):
+        r = 1.0 / (b[j] - a[j] * c[j - 1])
+        d[j] = r * (d[j] - a[j] * d[j - 1])
+        c[j] = r * c[j]
+        a[j] = -r * a[j] * a[j - 1]
+    for j in range(n - 3, 0, -1):
+        d[j] = d[j] - c[j] * d[j + 1]
+        a[j] = a[j] - c[j] * a[j + 1]
+        c[j] = -c[j] * c[j + 1]
+    r = 1.0 / (1.0 - a[1] * c[0])
+    d[0] = r * (d[0] - c[0] * d[1])
+    a[0] = r * a[0]
+    c[0] = -r * c[0] * c[1]
+    return (np.stack([a[0], a[n - 1]]), np.stack([c[0], c[n - 1]]), np.stack([d[0], d[n - 1]]))
+
+
+def tdma_update(a, c, d, x_rd):
+    """pascal_tdma.f90:595-605: the local rows from the reduced solution."""
+    n = d.shape[0]
+    d[0] = x_rd[0]
+    d[n - 1] = x_rd[1]
+    for j in range(1, n - 1):
+        d[j] = d[j] - a[j] * d[0] - c[j] * d[n - 1]

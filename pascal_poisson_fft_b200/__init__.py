@@ -47,7 +47,9 @@ EXPORTED_SYMBOLS = (
     "ppf_fft_poisson_plan_cuda_create", "ppf_cuda_poisson_fft_initial", "ppf_cuda_poisson_fft_1d",
     "ppf_cuda_poisson_fft_clean", "ppf_cuda_poisson_fft_set_precision", "ppf_stage_timing",
     "ppf_stage_times", "ppf_solve_noalloc", "ppf_solve_adjoint", "ppf_batch_create", "ppf_batch_destroy",
-    "ppf_batch_solve", "ppf_batch_info", "ppf_solve_host_async",
+    "ppf_batch_solve", "ppf_batch_info", "ppf_solve_host_async", "ppf_tdma_many_modified",
+    "ppf_tdma_many_update", "ppf_slab_systems", "ppf_slab_forward", "ppf_slab_coefficients",
+    "ppf_slab_inverse", "ppf_slab_sum", "ppf_slab_shift", "ppf_slab_ghosts",
 )
 PPF_BATCH_AUTOTUNE = 1
 STAGES = ("z-coefficients", "x-forward", "y-forward", "tdma-z", "y-inverse", "x-inverse",
@@ -93,6 +95,15 @@ def lib() -> ctypes.CDLL:
     L.ppf_plan_workspace_bytes.argtypes = [_vp, ctypes.POINTER(ctypes.c_longlong)]
     L.ppf_tdma_many.argtypes = [_vp] * 4 + [ctypes.c_int, ctypes.c_int, _vp]
     L.ppf_tdma_cycl_many.argtypes = [_vp] * 4 + [ctypes.c_int, ctypes.c_int, _vp]
+    L.ppf_tdma_many_modified.argtypes = [_vp] * 7 + [ctypes.c_int, ctypes.c_int, _vp]
+    L.ppf_tdma_many_update.argtypes = [_vp] * 4 + [ctypes.c_int, ctypes.c_int, _vp]
+    L.ppf_slab_systems.argtypes = [_vp, ctypes.POINTER(ctypes.c_int)]
+    L.ppf_slab_forward.argtypes = [_vp] * 3 + [_vp]
+    L.ppf_slab_coefficients.argtypes = [_vp] * 7 + [ctypes.c_int, ctypes.c_int, _vp]
+    L.ppf_slab_inverse.argtypes = [_vp] * 3 + [_vp]
+    L.ppf_slab_sum.argtypes = [_vp] * 3 + [_vp]
+    L.ppf_slab_shift.argtypes = [_vp] * 3 + [_vp]
+    L.ppf_slab_ghosts.argtypes = [_vp] * 5 + [ctypes.c_int, ctypes.c_int, _vp]
     L.ppf_fft_poisson_plan_cuda_create.argtypes = [ctypes.c_int] * 3 + [ctypes.c_double] * 3 + [ctypes.c_int] * 3
     L.ppf_cuda_poisson_fft_1d.argtypes = [_vp] * 6
     L.ppf_cuda_poisson_fft_set_precision.argtypes = [ctypes.c_int, ctypes.c_int]

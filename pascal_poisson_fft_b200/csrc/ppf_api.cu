@@ -133,6 +133,7 @@ struct ppf_plan {
     double* adj_red = nullptr;     // plane partial sums (5 * nz * nchunk), correction (nz), scratch (4 * nz)
     long adj_chunk = 0;
     int adj_nchunk = 0;
+    double* slab_part = nullptr;   // interior partial sums of ppf_slab_sum (allocated on first use)
     // per-stage timing (ppf_stage_timing)
     bool timing = false;
     std::vector<std::pair<int, cudaEvent_t>> marks;   // stage id (-1 = start), event
@@ -185,7 +186,7 @@ void free_plan(ppf_plan* p)
     if (!p) return;
     drop_marks(p);
     void* ptrs[] = { p->lamx, p->lamy, p->am, p->ap, p->scal, p->flags, p->tw,
-                     p->f_dev, p->p_dev, p->m_dev, p->adj_W, p->adj_red };
+                     p->f_dev, p->p_dev, p->m_dev, p->adj_W, p->adj_red, p->slab_part };
     for (void* q : ptrs)
         if (q) cudaFree(q);
     if (p->aux) cudaStreamDestroy(p->aux);
@@ -719,6 +720,143 @@ int ppf_tdma_cycl_many(const double* a, const double* b, const double* c, double
     if (n_row > 1025) return fail(PPF_ERR_UNSUPPORTED, "n_row %d > 1025", n_row);
     cudaError_t e = launch_tdma_many(a, b, c, d, n_sys, n_row, true, nullptr, (cudaStream_t)stream);
     if (e != cudaSuccess) return cuda_fail(e, "tdma_cycl_many");
+    return PPF_OK;
+}
+
+int ppf_tdma_many_modified(double* a, const double* b, double* c, double* d, double* a_rd, double* c_rd,
+                           double* d_rd, int n_sys, int n_row, void* stream)
+{
+    g_err[0] = 0;
+    if (!a || !b || !c || !d || !a_rd || !c_rd || !d_rd) return fail(PPF_ERR_INVALID, "null array argument");
+    if (n_sys < 1 || n_row < 3) return fail(PPF_ERR_INVALID, "n_sys %d must be >= 1 and n_row %d >= 3", n_sys, n_row);
+    cudaError_t e = launch_tdma_modified(a, b, c, d, a_rd, c_rd, d_rd, n_sys, n_row, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "tdma_many_modified");
+    return PPF_OK;
+}
+
+int ppf_tdma_many_update(const double* a, const double* c, double* d, const double* x_rd, int n_sys, int n_row,
+                         void* stream)
+{
+    g_err[0] = 0;
+    if (!a || !c || !d || !x_rd) return fail(PPF_ERR_INVALID, "null array argument");
+    if (n_sys < 1 || n_row < 3) return fail(PPF_ERR_INVALID, "n_sys %d must be >= 1 and n_row %d >= 3", n_sys, n_row);
+    cudaError_t e = launch_tdma_update(a, c, d, x_rd, n_sys, n_row, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "tdma_many_update");
+    return PPF_OK;
+}
+
+// ---- z-slab pieces of a multi-rank solve (the plan is this rank's slab) ----
+static int slab_plan(ppf_plan* p)
+{
+    g_err[0] = 0;
+    if (!p) return fail(PPF_ERR_INVALID, "null plan");
+    if (p->elem != 8) return fail(PPF_ERR_UNSUPPORTED, "z-slab solves run in FP64 (the reference's precision)");
+    int cur = -1;
+    PPF_CK(cudaGetDevice(&cur));
+    if (cur != p->dev) return fail(PPF_ERR_STATE, "plan was created on device %d, current device is %d", p->dev, cur);
+    return PPF_OK;
+}
+
+int ppf_slab_systems(const ppf_plan* plan, int* n_sys)
+{
+    if (!plan || !n_sys) return fail(PPF_ERR_INVALID, "null argument");
+    *n_sys = (int)((plan->cplx ? 2 : 1) * plan->b_pitch * (long)plan->my);
+    return PPF_OK;
+}
+
+int ppf_slab_forward(ppf_plan* plan, const double* f_d, double* spec_d, void* stream)
+{
+    int rc = slab_plan(plan);
+    if (rc != PPF_OK) return rc;
+    if (!f_d || !spec_d) return fail(PPF_ERR_INVALID, "null array argument");
+    ppf_plan* p = plan;
+    cudaStream_t st = (cudaStream_t)stream;
+    const cx<double>* tw = reinterpret_cast<const cx<double>*>(p->tw);
+    cudaError_t e = launch_xfwd<double>(p->xdct, f_d, nullptr, p->g, p->A, p->a_pitch, p->sx, tw + p->tw_off[0],
+                                        tw + p->tw_off[1], tw + p->tw_off[2], nullptr, st);
+    if (e != cudaSuccess) return cuda_fail(e, "slab x forward");
+    const long a_cp = p->xdct ? p->a_pitch / 2 : p->a_pitch;
+    const long b_cp = (p->xdct && p->ydct) ? p->b_pitch / 2 : p->b_pitch;
+    e = launch_yfwd<double>(p->ykind, reinterpret_cast<const cx<double>*>(p->A), a_cp,
+                            reinterpret_cast<cx<double>*>(spec_d), b_cp, p->ycols, p->g, p->sy, tw + p->tw_off[3],
+                            tw + p->tw_off[4], nullptr, st);
+    if (e != cudaSuccess) return cuda_fail(e, "slab y forward");
+    return PPF_OK;
+}
+
+int ppf_slab_coefficients(ppf_plan* plan, double* a_d, double* b_d, double* c_d, double* spec_d,
+                          const double* dx3_g, const double* dmx3_g, int z0, int n3m_g, void* stream)
+{
+    int rc = slab_plan(plan);
+    if (rc != PPF_OK) return rc;
+    if (!a_d || !b_d || !c_d || !spec_d || !dx3_g || !dmx3_g) return fail(PPF_ERR_INVALID, "null array argument");
+    if (z0 < 0 || z0 + plan->g.nz > n3m_g) return fail(PPF_ERR_INVALID, "slab rows %d..%d outside 0..%d", z0,
+                                                       z0 + plan->g.nz, n3m_g);
+    int ns = 0;
+    ppf_slab_systems(plan, &ns);
+    cudaError_t e = launch_slab_coef(a_d, b_d, c_d, spec_d, ns, plan->g.nz, plan->cplx ? 1 : 0, plan->b_pitch,
+                                     plan->mx, plan->lamx, plan->lamy, dx3_g, dmx3_g, z0, n3m_g, plan->scale,
+                                     (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "slab coefficients");
+    return PPF_OK;
+}
+
+int ppf_slab_inverse(ppf_plan* plan, const double* spec_d, double* p_d, void* stream)
+{
+    int rc = slab_plan(plan);
+    if (rc != PPF_OK) return rc;
+    if (!spec_d || !p_d) return fail(PPF_ERR_INVALID, "null array argument");
+    ppf_plan* p = plan;
+    cudaStream_t st = (cudaStream_t)stream;
+    const cx<double>* tw = reinterpret_cast<const cx<double>*>(p->tw);
+    const long a_cp = p->xdct ? p->a_pitch / 2 : p->a_pitch;
+    const long b_cp = (p->xdct && p->ydct) ? p->b_pitch / 2 : p->b_pitch;
+    cudaError_t e = launch_yinv<double>(p->ykind, reinterpret_cast<const cx<double>*>(spec_d), b_cp,
+                                        reinterpret_cast<cx<double>*>(p->A), a_cp, p->ycols, p->g, p->sy,
+                                        tw + p->tw_off[3], tw + p->tw_off[4], nullptr, nullptr, st);
+    if (e != cudaSuccess) return cuda_fail(e, "slab y inverse");
+    e = launch_xinv<double>(p->xdct, p->A, p->a_pitch, p_d, p->g, false, false, nullptr, nullptr, p->sx,
+                            tw + p->tw_off[0], tw + p->tw_off[1], tw + p->tw_off[2], nullptr, st);
+    if (e != cudaSuccess) return cuda_fail(e, "slab x inverse");
+    return PPF_OK;
+}
+
+int ppf_slab_sum(ppf_plan* plan, const double* p_d, double* sum_d, void* stream)
+{
+    int rc = slab_plan(plan);
+    if (rc != PPF_OK) return rc;
+    if (!p_d || !sum_d) return fail(PPF_ERR_INVALID, "null array argument");
+    if (!plan->slab_part) {
+        if (cudaMalloc(&plan->slab_part, sizeof(double) * slab_sum_parts(plan->g)) != cudaSuccess) {
+            cudaGetLastError();
+            plan->slab_part = nullptr;
+            return fail(PPF_ERR_NOMEM, "cannot allocate the slab reduction");
+        }
+    }
+    cudaError_t e = launch_slab_sum(p_d, plan->g, plan->slab_part, sum_d, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "slab sum");
+    return PPF_OK;
+}
+
+int ppf_slab_shift(ppf_plan* plan, double* p_d, const double* shift_d, void* stream)
+{
+    int rc = slab_plan(plan);
+    if (rc != PPF_OK) return rc;
+    if (!p_d || !shift_d) return fail(PPF_ERR_INVALID, "null array argument");
+    cudaError_t e = launch_slab_shift(p_d, plan->g, shift_d, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "slab shift");
+    return PPF_OK;
+}
+
+int ppf_slab_ghosts(ppf_plan* plan, double* p_d, const double* dmx1_d, const double* dmx2_d, const double* dmx3_d,
+                    int z_lo_wall, int z_hi_wall, void* stream)
+{
+    int rc = slab_plan(plan);
+    if (rc != PPF_OK) return rc;
+    if (!p_d || !dmx1_d || !dmx2_d || !dmx3_d) return fail(PPF_ERR_INVALID, "null array argument");
+    const int zf = plan->g.pz ? 0 : ((z_lo_wall ? 1 : 0) | (z_hi_wall ? 2 : 0));
+    cudaError_t e = launch_ghosts(p_d, plan->g, dmx1_d, dmx2_d, dmx3_d, (cudaStream_t)stream, zf);
+    if (e != cudaSuccess) return cuda_fail(e, "slab ghost cells");
     return PPF_OK;
 }
 

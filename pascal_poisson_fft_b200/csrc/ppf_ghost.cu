@@ -15,7 +15,7 @@
 namespace ppf {
 
 __global__ void k_ghost_axis(double* __restrict__ P, int dir, int neumann, int n1m, int n2m, int n3m,
-                             long sy, long sz, const double* __restrict__ dmx)
+                             long sy, long sz, const double* __restrict__ dmx, int faces)
 {
     const int N1 = n1m + 2, N2 = n2m + 2, N3 = n3m + 2;
     int nb, nm;
@@ -39,8 +39,8 @@ __global__ void k_ghost_axis(double* __restrict__ P, int dir, int neumann, int n
         const long ib = idx % nb, ic = idx / nb;
         const long base = ib * sb + ic * sc;
         if (neumann) {
-            P[base] = alo * P[base + sa] - blo * P[base + 2 * sa];
-            P[base + na * sa] = ahi * P[base + nm * sa] - bhi * P[base + (na - 2) * sa];
+            if (faces & 1) P[base] = alo * P[base + sa] - blo * P[base + 2 * sa];
+            if (faces & 2) P[base + na * sa] = ahi * P[base + nm * sa] - bhi * P[base + (na - 2) * sa];
         } else {
             const double v0 = P[base + sa], v1 = P[base + nm * sa];
             P[base] = v1;
@@ -50,7 +50,7 @@ __global__ void k_ghost_axis(double* __restrict__ P, int dir, int neumann, int n
 }
 
 cudaError_t launch_ghosts(double* P, const Geom& g, const double* dmx1, const double* dmx2, const double* dmx3,
-                          cudaStream_t st)
+                          cudaStream_t st, int zfaces)
 {
     const int per[3] = { g.px, g.py, g.pz };
     const double* dmx[3] = { dmx1, dmx2, dmx3 };
@@ -60,9 +60,13 @@ cudaError_t launch_ghosts(double* P, const Geom& g, const double* dmx1, const do
         for (int d = 0; d < 3; ++d) {
             const bool neumann = !per[d];
             if ((pass == 0) != neumann) continue;
+            // z of a slab: walls only at the global ends (zfaces), the
+            // planes between slabs come from the neighbouring ranks
+            const int faces = (d == 2) ? zfaces : 3;
+            if (faces == 0) continue;
             const int blocks = (int)((face[d] + 255) / 256);
             k_ghost_axis<<<blocks, 256, 0, st>>>(P, d, neumann ? 1 : 0, g.nx, g.ny, g.nz, g.pstride_y,
-                                                 g.pstride_z, dmx[d]);
+                                                 g.pstride_z, dmx[d], faces);
             cudaError_t e = cudaGetLastError();
             if (e != cudaSuccess) return e;
         }

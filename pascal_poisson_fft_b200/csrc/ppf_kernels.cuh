@@ -94,12 +94,28 @@ cudaError_t launch_zcoef(const double* dx3, const double* dmx3, int nz, double* 
                          double* dzmax2, cudaStream_t st);
 
 // ---- ghost cells (ppf_ghost.cu) ----
+// zfaces: z faces to fill (1 lower, 2 upper; 3 for a whole domain, the
+// ends of a z slab that are global walls for a slab)
 cudaError_t launch_ghosts(double* P, const Geom& g, const double* dmx1, const double* dmx2,
-                          const double* dmx3, cudaStream_t st);
+                          const double* dmx3, cudaStream_t st, int zfaces = 3);
+
+// ---- z-slab pieces of the multi-rank solve (ppf_slab.cu) ----
+cudaError_t launch_slab_coef(double* a, double* b, double* c, double* d, long ns, int nzl, int cplx, long pitch,
+                             int mx, const double* lamx, const double* lamy, const double* dx3, const double* dmx3,
+                             int z0, int nzg, double scale, cudaStream_t st);
+long slab_sum_parts(const Geom& g);
+cudaError_t launch_slab_sum(const double* P, const Geom& g, double* part, double* sum, cudaStream_t st);
+cudaError_t launch_slab_shift(double* P, const Geom& g, const double* shift, cudaStream_t st);
 
 // ---- generic batched TDMA on coefficient arrays (ppf_tdma.cu) ----
 cudaError_t launch_tdma_many(const double* a, const double* b, const double* c, double* d,
                              int n_sys, int n_row, bool cyclic, int* err, cudaStream_t st);
+
+// ---- rows split over ranks: PaScaL modified Thomas and update (ppf_tdma.cu) ----
+cudaError_t launch_tdma_modified(double* a, const double* b, double* c, double* d, double* a_rd, double* c_rd,
+                                 double* d_rd, long n_sys, int n_row, cudaStream_t st);
+cudaError_t launch_tdma_update(const double* a, const double* c, double* d, const double* x_rd, long n_sys, int n_row,
+                               cudaStream_t st);
 
 // Refinement bookkeeping after an x-inverse pass with partials: reduces the
 // partials in a fixed order, stores mean(u) for the next accumulate pass,

@@ -717,6 +717,99 @@ cudaError_t launch_tdma_many(const double* a, const double* b, const double* c, 
     return cudaGetLastError();
 }
 
+// --------------------------------------------------------------------------
+// Rows of the systems split over ranks (z slabs): PaScaL's modified Thomas
+// algorithm (01_Fortran/PaScaL_TDMA/src/pascal_tdma_cuda.f90:332-473).  Each
+// rank eliminates its local rows so that every row depends only on its own
+// unknown and on the unknowns of the rank's first and last rows; those two
+// rows form the rank's part of a reduced system of 2 * nranks rows per
+// system (b = 1), which the caller gathers, solves and scatters back, and
+// k_tdma_update finishes the local rows (:483-520).  The arithmetic follows
+// the reference operation for operation (rounding-explicit, as in the
+// single-rank kernels).  Layout: element (sys, row) at [row * n_sys + sys];
+// reduced rows (sys, r) at [r * n_sys + sys], r = 0 (first row), 1 (last).
+// --------------------------------------------------------------------------
+__global__ void __launch_bounds__(TPB) k_tdma_modified(double* __restrict__ a, const double* __restrict__ b,
+                                                       double* __restrict__ c, double* __restrict__ d,
+                                                       double* __restrict__ a_rd, double* __restrict__ c_rd,
+                                                       double* __restrict__ d_rd, long ns, int n)
+{
+    const long s = (long)blockIdx.x * TPB + threadIdx.x;
+    if (s >= ns) return;
+    using X = Exact;
+    auto at = [&](int i) { return (long)i * ns + s; };
+    // rows 1 and 2 are normalised by their diagonal
+    double a0 = X::div(a[at(0)], b[at(0)]), c0 = X::div(c[at(0)], b[at(0)]), d0 = X::div(d[at(0)], b[at(0)]);
+    a[at(0)] = a0; c[at(0)] = c0; d[at(0)] = d0;
+    double a1 = X::div(a[at(1)], b[at(1)]), c1 = X::div(c[at(1)], b[at(1)]), d1 = X::div(d[at(1)], b[at(1)]);
+    a[at(1)] = a1; c[at(1)] = c1; d[at(1)] = d1;
+    // elimination of the lower diagonal, rows 3..n
+    for (int i = 2; i < n; ++i) {
+        a0 = a1; c0 = c1; d0 = d1;
+        const double ai = a[at(i)], bi = b[at(i)], ci = c[at(i)], di = d[at(i)];
+        const double r = X::div(1.0, X::sub(bi, X::mul(ai, c0)));
+        d1 = X::mul(r, X::sub(di, X::mul(ai, d0)));
+        c1 = X::mul(r, ci);
+        a1 = X::mul(X::mul(-r, ai), a0);
+        a[at(i)] = a1; c[at(i)] = c1; d[at(i)] = d1;
+    }
+    a_rd[ns + s] = a1;
+    c_rd[ns + s] = c1;
+    d_rd[ns + s] = d1;
+    // elimination of the upper diagonal, rows n-2..2, from row n-1
+    a1 = a0; c1 = c0; d1 = d0;
+    for (int i = n - 3; i >= 1; --i) {
+        double ai = a[at(i)], ci = c[at(i)], di = d[at(i)];
+        di = X::sub(di, X::mul(ci, d1));
+        ai = X::sub(ai, X::mul(ci, a1));
+        ci = X::mul(-ci, c1);
+        a1 = ai; c1 = ci; d1 = di;
+        a[at(i)] = ai; c[at(i)] = ci; d[at(i)] = di;
+    }
+    {
+        double ai = a[at(0)], ci = c[at(0)], di = d[at(0)];
+        const double r = X::div(1.0, X::sub(1.0, X::mul(a1, ci)));
+        di = X::mul(r, X::sub(di, X::mul(ci, d1)));
+        ai = X::mul(r, ai);
+        ci = X::mul(X::mul(-r, ci), c1);
+        a[at(0)] = ai; c[at(0)] = ci; d[at(0)] = di;
+        a_rd[s] = ai;
+        c_rd[s] = ci;
+        d_rd[s] = di;
+    }
+}
+
+__global__ void __launch_bounds__(TPB) k_tdma_update(const double* __restrict__ a, const double* __restrict__ c,
+                                                     double* __restrict__ d, const double* __restrict__ x_rd, long ns,
+                                                     int n)
+{
+    const long s = (long)blockIdx.x * TPB + threadIdx.x;
+    if (s >= ns) return;
+    const double xs = x_rd[s], xe = x_rd[ns + s];
+    d[s] = xs;
+    d[(long)(n - 1) * ns + s] = xe;
+    for (int i = 1; i < n - 1; ++i) {
+        const long o = (long)i * ns + s;
+        d[o] = __dsub_rn(__dsub_rn(d[o], __dmul_rn(a[o], xs)), __dmul_rn(c[o], xe));
+    }
+}
+
+cudaError_t launch_tdma_modified(double* a, const double* b, double* c, double* d, double* a_rd, double* c_rd,
+                                 double* d_rd, long n_sys, int n_row, cudaStream_t st)
+{
+    dim3 grid((unsigned)((n_sys + TPB - 1) / TPB));
+    k_tdma_modified<<<grid, TPB, 0, st>>>(a, b, c, d, a_rd, c_rd, d_rd, n_sys, n_row);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tdma_update(const double* a, const double* c, double* d, const double* x_rd, long n_sys, int n_row,
+                               cudaStream_t st)
+{
+    dim3 grid((unsigned)((n_sys + TPB - 1) / TPB));
+    k_tdma_update<<<grid, TPB, 0, st>>>(a, c, d, x_rd, n_sys, n_row);
+    return cudaGetLastError();
+}
+
 // z coefficients of cuda_Poisson_TDMA_z_* (fft_3d_poisson.f90:1139-1142):
 // am_k = 1/dx3_k/dmx3_k, ap_k = 1/dx3_k/dmx3_{k+1}, am_1 = ap_n3m = 0; plus
 // max_k dx3_k^2 for the low-wavenumber precision switch.  One CTA.
