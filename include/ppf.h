@@ -55,8 +55,9 @@ typedef struct {
     int max_sweeps;            /* PPF_MIXED: FP64-residual refinement sweeps after the
                                   first FP32 solve (0..8); <0 selects the default (2) */
     double sweep_tol;          /* PPF_MIXED: stop refining once ||du||/||u|| < tol (0 = never) */
-    double lowk_threshold;     /* FP32 TDMA rows with lambda*dz_max^2 below this run in FP64
-                                  (<=0 selects the default 1e-3) */
+    double lowk_threshold;     /* FP32 storage: z systems with lambda*dz_min^2 below this (the
+                                  near-singular low wavenumbers, k^2 dz^2 << 1 at the finest
+                                  z spacing) are solved in FP64 (<=0 selects the default 1e-3) */
 } ppf_desc;
 
 /* Create / destroy a plan on the current CUDA device.  Allocates the

@@ -110,7 +110,7 @@ struct ppf_plan {
     double* lamy = nullptr;
     double* am = nullptr;
     double* ap = nullptr;
-    double* scal = nullptr;    // [0] dzmax2, [3] last ||du||/||u||, [4] zero-mode shift, [5] mean of the iterate
+    double* scal = nullptr;    // [0] min dz^2, [3] last ||du||/||u||, [4] zero-mode shift, [5] mean of the iterate
     int* flags = nullptr;      // [0] skip, [1] sweeps_done, [2] err
     double* partials = nullptr;  // per-block sums of the x-inverse pass (mixed precision)
     long xinv_nblk = 0;
@@ -363,7 +363,7 @@ int run_pass(ppf_plan* p, const double* f, double* P, bool resid, bool accumulat
     z.mx = p->mx; z.my = p->my; z.pitch = p->b_pitch; z.plane = p->b_pitch * (long)p->my; z.nz = p->g.nz;
     z.lamx = p->lamx; z.lamy = p->lamy; z.am = p->am; z.ap = p->ap; z.scale = p->scale;
     z.lowk = (p->d.precision == PPF_FP64) ? 0.0 : p->d.lowk_threshold;
-    z.dzmax2 = p->scal;
+    z.dzmin2 = p->scal;
     z.dc_shift = p->scal + 4;
     z.cyclic = p->g.pz;
     z.ckpt = p->ckpt;

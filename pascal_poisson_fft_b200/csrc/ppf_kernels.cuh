@@ -65,8 +65,8 @@ struct ZSys {
     const double* am;     // z coefficient tables (nz)
     const double* ap;
     double scale;         // normalisation folded into the solution
-    double lowk;          // FP32 storage: systems with lam*dzmax^2 < lowk solve in FP64
-    const double* dzmax2; // device scalar: max_k dx3_k^2 (written by the z-coefficient kernel)
+    double lowk;          // FP32 storage: systems with lam*dz_min^2 < lowk solve in FP64
+    const double* dzmin2; // device scalar: min_k dx3_k^2 (written by the z-coefficient kernel)
     double* dc_shift;     // device scalar: z-average of the (0,0) solution (subtracted by the y inverse)
     int cyclic;           // periodic z: the reference's cyclic Thomas sequence
     double* ckpt;         // Thomas checkpoints, tdma_z_ckpt_doubles(nz, plane, cyclic, fp32) doubles
@@ -91,7 +91,7 @@ template <typename T, bool CPLX>
 cudaError_t launch_tdma_z(void* data, const ZSys& z, const int* skip_flag, int* err_flag, const ZStreams& zs);
 
 cudaError_t launch_zcoef(const double* dx3, const double* dmx3, int nz, double* am, double* ap,
-                         double* dzmax2, cudaStream_t st);
+                         double* dzmin2, cudaStream_t st);
 
 // ---- ghost cells (ppf_ghost.cu) ----
 // zfaces: z faces to fill (1 lower, 2 upper; 3 for a whole domain, the

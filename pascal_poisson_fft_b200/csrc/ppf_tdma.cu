@@ -361,7 +361,7 @@ __global__ void __launch_bounds__(TPB) k_thomas_z(void* __restrict__ data_, ZSys
     co.ly = z.lamy[ky];
     co.pin = (kx == 0 && ky == 0);
     if (MODE != 0) {
-        const bool low = (co.lx + co.ly) * __ldg(z.dzmax2) < z.lowk;
+        const bool low = (co.lx + co.ly) * __ldg(z.dzmin2) < z.lowk;
         if ((MODE == 1) == low) return;
     }
     double zsum = 0.0;
@@ -389,7 +389,7 @@ float* tdma_z_ckpt_f32(double* ckpt, int nz, long plane, int cyclic)
 }
 
 namespace {
-// FP32 bulk of the mixed-precision z solve (systems with lam dz_max^2 >=
+// FP32 bulk of the mixed-precision z solve (systems with lam dz_min^2 >=
 // lowk, non-periodic z).  The same Thomas sweep as thomas_poisson<Fast>,
 // with the level coefficients (am, ap, -am-ap) staged once per CTA in shared
 // memory (b = -am-ap - lam, a single rounding more than the FP64 order,
@@ -411,7 +411,7 @@ __global__ void __launch_bounds__(TPB) k_thomas_fast(void* __restrict__ data_, Z
     const int kx = (int)(sys % z.pitch), ky = (int)(sys / z.pitch);
     if (kx >= z.mx || ky >= z.my) return;
     const double lam = z.lamx[kx] + z.lamy[ky];
-    if (lam * __ldg(z.dzmax2) < z.lowk) return;  // solved in FP64 (includes the pinned zero mode)
+    if (lam * __ldg(z.dzmin2) < z.lowk) return;  // solved in FP64 (includes the pinned zero mode)
     const float lamf = (float)lam, sc = (float)z.scale;
     const int nz = z.nz;
     const long plane = z.plane;
@@ -812,13 +812,14 @@ cudaError_t launch_tdma_update(const double* a, const double* c, double* d, cons
 
 // z coefficients of cuda_Poisson_TDMA_z_* (fft_3d_poisson.f90:1139-1142):
 // am_k = 1/dx3_k/dmx3_k, ap_k = 1/dx3_k/dmx3_{k+1}, am_1 = ap_n3m = 0; plus
-// max_k dx3_k^2 for the low-wavenumber precision switch.  One CTA.
+// min_k dx3_k^2 for the low-wavenumber precision switch (a system is
+// near-singular when lam dz^2 << 1 at the finest spacing).  One CTA.
 __global__ void __launch_bounds__(256) k_zcoef(const double* __restrict__ dx3, const double* __restrict__ dmx3,
                                                int nz, double* __restrict__ am, double* __restrict__ ap,
-                                               double* __restrict__ dzmax2)
+                                               double* __restrict__ dzmin2)
 {
     __shared__ double red[256];
-    double mx = 0.0;
+    double mn = INFINITY;
     for (int k = threadIdx.x; k < nz; k += blockDim.x) {
         const int kk = k + 1;
         double av = __ddiv_rn(__ddiv_rn(1.0, dx3[kk]), dmx3[kk]);
@@ -827,21 +828,21 @@ __global__ void __launch_bounds__(256) k_zcoef(const double* __restrict__ dx3, c
         if (k == nz - 1) cv = 0.0;
         am[k] = av;
         ap[k] = cv;
-        mx = fmax(mx, dx3[kk] * dx3[kk]);
+        mn = fmin(mn, dx3[kk] * dx3[kk]);
     }
-    red[threadIdx.x] = mx;
+    red[threadIdx.x] = mn;
     __syncthreads();
     for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-        if (threadIdx.x < o) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + o]);
+        if (threadIdx.x < o) red[threadIdx.x] = fmin(red[threadIdx.x], red[threadIdx.x + o]);
         __syncthreads();
     }
-    if (threadIdx.x == 0) *dzmax2 = red[0];
+    if (threadIdx.x == 0) *dzmin2 = red[0];
 }
 
-cudaError_t launch_zcoef(const double* dx3, const double* dmx3, int nz, double* am, double* ap, double* dzmax2,
+cudaError_t launch_zcoef(const double* dx3, const double* dmx3, int nz, double* am, double* ap, double* dzmin2,
                          cudaStream_t st)
 {
-    k_zcoef<<<1, 256, 0, st>>>(dx3, dmx3, nz, am, ap, dzmax2);
+    k_zcoef<<<1, 256, 0, st>>>(dx3, dmx3, nz, am, ap, dzmin2);
     return cudaGetLastError();
 }
 
