@@ -495,11 +495,142 @@ __global__ void __launch_bounds__(TPB) k_thomas_fast(void* __restrict__ data_, Z
     if (bad && err) atomicOr(err, 1);
 }
 
+
+// FP64 z solve of all systems (non-periodic z): thomas_poisson<Exact> with
+// the level coefficients staged once per CTA in shared memory (the same
+// rounded operations: b = ((-am - ap) - lx) - ly with -am - ap kept per
+// level) and, with PREF, the next chunk's rows loaded while the current one
+// is eliminated.
+template <bool CPLX, bool PREF>
+__global__ void __launch_bounds__(TPB) k_thomas_exact(void* __restrict__ data_, ZSys z, const int* __restrict__ skip,
+                                                      int* __restrict__ err)
+{
+    if (skip && *skip) return;
+    extern __shared__ double zl[];     // am[nz], ap[nz], s[nz] = -am - ap
+    const int nz = z.nz;
+    for (int k = threadIdx.x; k < nz; k += TPB) {
+        const double am = z.am[k], ap = z.ap[k];
+        zl[k] = am;
+        zl[nz + k] = ap;
+        zl[2 * nz + k] = __dsub_rn(-am, ap);
+    }
+    __syncthreads();
+    using E = typename Elem<double, CPLX>::type;
+    using X = Exact;
+    const long sys = (long)blockIdx.x * TPB + threadIdx.x;
+    const int kx = (int)(sys % z.pitch), ky = (int)(sys / z.pitch);
+    if (kx >= z.mx || ky >= z.my) return;
+    const double lx = z.lamx[kx], ly = z.lamy[ky];
+    const bool pin = (kx == 0 && ky == 0);
+    const long plane = z.plane;
+    constexpr int C = Exact::CH;
+    const int nch = (nz + C - 1) / C;
+    E* col = reinterpret_cast<E*>(data_) + sys;
+    double* ck = z.ckpt + sys;
+    auto coef = [&](int zr, double& a, double& b, double& c) {
+        if (pin && zr == 0) { a = 0.0; b = 1.0; c = 0.0; return; }
+        a = zl[zr];
+        c = zl[nz + zr];
+        b = X::sub(X::sub(zl[2 * nz + zr], lx), ly);
+    };
+    double nr[C], ni[C];
+    auto load = [&](int z0) {
+#pragma unroll
+        for (int q = 0; q < C; ++q) {
+            nr[q] = 0.0; ni[q] = 0.0;
+            if (z0 + q < nz) ld_cv<double, double>(col + (long)(z0 + q) * plane, nr[q], ni[q]);
+        }
+    };
+    if (PREF) load(0);
+    double cp = 0, dr = 0, di = 0;
+    for (int ch = 0; ch < nch; ++ch) {
+        const int z0 = ch * C;
+        double vr[C], vi[C];
+        if (PREF) {
+#pragma unroll
+            for (int q = 0; q < C; ++q) { vr[q] = nr[q]; vi[q] = ni[q]; }
+            if (ch + 1 < nch) load((ch + 1) * C);
+        } else {
+            load(z0);
+#pragma unroll
+            for (int q = 0; q < C; ++q) { vr[q] = nr[q]; vi[q] = ni[q]; }
+        }
+#pragma unroll
+        for (int q = 0; q < C; ++q) {
+            const int zr = z0 + q;
+            if (zr < nz) {
+                double a, b, c;
+                coef(zr, a, b, c);
+                const bool pr = pin && zr == 0;
+                fwd_row<Exact, CPLX>(zr == 0, a, b, c, pr ? 0.0 : vr[q], pr ? 0.0 : vi[q], cp, dr, di);
+            }
+        }
+        double* c3 = ck + (long)(3 * ch) * plane;
+        c3[0] = cp;
+        c3[plane] = dr;
+        if (CPLX) c3[2 * plane] = di;
+    }
+    double xr = 0, xi = 0, zsum = 0.0;
+    bool bad = false;
+    if (PREF) load((nch - 1) * C);
+    for (int ch = nch - 1; ch >= 0; --ch) {
+        const int z0 = ch * C;
+        double vr[C], vi[C], c_[C];
+        double pcp = 0, pdr = 0, pdi = 0;
+        if (PREF) {
+#pragma unroll
+            for (int q = 0; q < C; ++q) { vr[q] = nr[q]; vi[q] = ni[q]; }
+        } else {
+            load(z0);
+#pragma unroll
+            for (int q = 0; q < C; ++q) { vr[q] = nr[q]; vi[q] = ni[q]; }
+        }
+        if (ch > 0) {
+            const double* c3 = ck + (long)(3 * (ch - 1)) * plane;
+            pcp = c3[0];
+            pdr = c3[plane];
+            if (CPLX) pdi = c3[2 * plane];
+            if (PREF) load((ch - 1) * C);
+        }
+#pragma unroll
+        for (int q = 0; q < C; ++q) {
+            const int zr = z0 + q;
+            if (zr < nz) {
+                double a, b, c;
+                coef(zr, a, b, c);
+                const bool pr = pin && zr == 0;
+                fwd_row<Exact, CPLX>(zr == 0, a, b, c, pr ? 0.0 : vr[q], pr ? 0.0 : vi[q], pcp, pdr, pdi);
+            }
+            c_[q] = pcp; vr[q] = pdr; vi[q] = pdi;
+        }
+#pragma unroll
+        for (int q = C - 1; q >= 0; --q) {
+            const int zr = z0 + q;
+            if (zr < nz) {
+                if (zr == nz - 1) {
+                    xr = vr[q];
+                    xi = vi[q];
+                } else {
+                    xr = X::sub(vr[q], X::mul(c_[q], xr));
+                    if (CPLX) xi = X::sub(vi[q], X::mul(c_[q], xi));
+                }
+                const double sr = xr * z.scale, si = xi * z.scale;
+                zsum += sr;
+                if (!isfinite(sr) || !isfinite(si)) bad = true;
+                st_elem<double>(col + (long)zr * plane, sr, si);
+            }
+        }
+    }
+    if (pin && z.dc_shift) *z.dc_shift = zsum / (double)nz;
+    if (bad && err) atomicOr(err, 1);
+}
+
 template <bool CPLX, bool CYC>
 cudaError_t launch_z(double*, const ZSys& z, void* data, const int* skip, int* err, const ZStreams& zs)
 {
     dim3 grid((unsigned)((z.plane + TPB - 1) / TPB));  // pitch * my systems incl. padding columns
-    k_thomas_z<double, Exact, CPLX, 0, CYC><<<grid, TPB, 0, zs.st>>>(data, z, skip, err);
+    if (CYC) k_thomas_z<double, Exact, CPLX, 0, CYC><<<grid, TPB, 0, zs.st>>>(data, z, skip, err);
+    else k_thomas_exact<CPLX, true><<<grid, TPB, 3 * sizeof(double) * z.nz, zs.st>>>(data, z, skip, err);
     return cudaGetLastError();
 }
 // FP32 data: the bulk in FP32 and, concurrently on the auxiliary stream when
