@@ -70,7 +70,8 @@ def max_over_ranks(value: float, ws: int, device=None) -> float:
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms while running."""
+    """nvidia-smi clocks / throttle reasons sampled every 50 ms while running
+    (start() returns once the first sample is in, so the timed region is covered)."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -84,13 +85,16 @@ class ClockSampler:
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                                          "-lms", "200", "-i", str(self.gpu)],
+                                          "-lms", "50", "-i", str(self.gpu)],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except (OSError, FileNotFoundError):
             self.proc = None
             return
         self.th = threading.Thread(target=self._read, daemon=True)
         self.th.start()
+        t0 = time.time()
+        while not self.rows and time.time() - t0 < 3.0:
+            time.sleep(0.01)
 
     def _read(self):
         for line in self.proc.stdout:
@@ -101,7 +105,7 @@ class ClockSampler:
     def stop(self):
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
-        time.sleep(0.25)
+        time.sleep(0.06)
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
@@ -273,47 +277,51 @@ def run_ours(args, ws, rank, lrank):
 
     # end to end through the host-array C ABI: every step copies f in from
     # page-locked host memory, solves and copies P out (ppf_solve_host_async).
-    # Two plans alternate on two streams, so one step's copy-out overlaps
-    # the next step's copy-in (separate copy engines); the timed region
-    # spans all K steps and every copy.
+    # Three plans take turns on three streams, so the copy engines stay busy:
+    # one step's copy-out overlaps the next steps' copy-in (separate engines),
+    # and a stream's next copy-in does not wait behind its own copy-out.  The
+    # timed region spans all K steps and every copy.
     e2e = None
     if not args.no_e2e:
-        planm2 = ppf.Plan(n1, n2, n3, p.L1, p.L2, *p.pbc, precision=ppf.PPF_MIXED, max_sweeps=sweeps)
-        plans = (planm, planm2)
-        streams = (torch.cuda.Stream(device=dev), torch.cuda.Stream(device=dev))
+        NP = 3
+        plans = [planm] + [ppf.Plan(n1, n2, n3, p.L1, p.L2, *p.pbc, precision=ppf.PPF_MIXED, max_sweeps=sweeps)
+                           for _ in range(NP - 1)]
+        streams = [torch.cuda.Stream(device=dev) for _ in range(NP)]
         fh = torch.empty(f.shape, dtype=torch.float64, pin_memory=True)
         fh.copy_(f)
-        Ph = [torch.empty(P.shape, dtype=torch.float64, pin_memory=True) for _ in range(2)]
+        Ph = [torch.empty(P.shape, dtype=torch.float64, pin_memory=True) for _ in range(NP)]
         mh = [torch.as_tensor(np.ascontiguousarray(m[k])).pin_memory() for k in ("dmx1", "dmx2", "dmx3", "dx3")]
 
         def e2e_steps(k, e_start=None, e_ends=None):
             if e_start is not None:
                 e_start.record(streams[0])
-                streams[1].wait_event(e_start)
+                for sm in streams[1:]:
+                    sm.wait_event(e_start)
             for i in range(k):
-                plans[i % 2].solve_host_async(fh, Ph[i % 2], *mh, stream=streams[i % 2])
+                plans[i % NP].solve_host_async(fh, Ph[i % NP], *mh, stream=streams[i % NP])
             if e_ends is not None:
                 for ev, sm in zip(e_ends, streams):
                     ev.record(sm)
 
-        e2e_steps(max(2, min(args.warmup, 4)))
+        e2e_steps(max(NP, min(args.warmup, 6)))
         torch.cuda.synchronize()
-        k2 = max(4, min(args.steps, 12))
+        k2 = max(2 * NP, min(args.steps, 12))
         if ws > 1:
             torch.distributed.barrier()
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
-        ends = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(NP)]
         e2e_steps(k2, e0, ends)
         torch.cuda.synchronize()
         ms_e2e = max_over_ranks(max(e0.elapsed_time(ev) for ev in ends) / k2, ws, dev)
         # the last step's result matches the device solve of the same input
-        e2e_rel = float(torch.linalg.vector_norm(Ph[(k2 - 1) % 2].to(dev) - P64) / torch.linalg.vector_norm(P64))
+        e2e_rel = float(torch.linalg.vector_norm(Ph[(k2 - 1) % NP].to(dev) - P64) / torch.linalg.vector_norm(P64))
         h2d = fh.nbytes + sum(a.nbytes for a in mh)
         e2e = {"value": ws * 1000.0 / ms_e2e, "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(Ph[0].nbytes), "ms_per_step": ms_e2e,
-               "api": "ppf_solve_host_async, two plans on two streams", "rel_l2_vs_fp64": e2e_rel}
-        planm2.close()
+               "api": f"ppf_solve_host_async, {NP} plans on {NP} streams", "rel_l2_vs_fp64": e2e_rel}
+        for q in plans[1:]:
+            q.close()
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
