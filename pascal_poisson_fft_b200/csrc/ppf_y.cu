@@ -179,11 +179,9 @@ __global__ void __launch_bounds__(512) k_yinv(const cx<T>* __restrict__ in, long
 // is transformed and stored, so the loads of one tile overlap the
 // butterflies of the previous one.
 template <typename T, bool INV, typename SH>
-__global__ void __launch_bounds__(SH::NT) k_y_c2c_pipe(const cx<T>* __restrict__ in, long in_pitch,
-                                                      cx<T>* __restrict__ out, long out_pitch, int ncols, int nz,
-                                                      const cx<T>* __restrict__ tw,
-                                                      const double* __restrict__ dc_shift,
-                                                      const int* __restrict__ skip)
+__device__ __forceinline__ void y_c2c_pipe(const cx<T>* __restrict__ in, long in_pitch, cx<T>* __restrict__ out,
+                                           long out_pitch, int ncols, int nz, const cx<T>* __restrict__ tw,
+                                           const double* __restrict__ dc_shift, const int* __restrict__ skip)
 {
     if (skip && *skip) return;
     constexpr int N = SH::N, W = SH::W, NT = SH::NT;
@@ -235,9 +233,32 @@ __global__ void __launch_bounds__(SH::NT) k_y_c2c_pipe(const cx<T>* __restrict__
     }
 }
 
+// FP32 tiles: one CTA per SM (two 64 KB buffers at 512 threads)
+template <typename T, bool INV, typename SH>
+__global__ void __launch_bounds__(SH::NT) k_y_c2c_pipe(const cx<T>* __restrict__ in, long in_pitch,
+                                                      cx<T>* __restrict__ out, long out_pitch, int ncols, int nz,
+                                                      const cx<T>* __restrict__ tw,
+                                                      const double* __restrict__ dc_shift,
+                                                      const int* __restrict__ skip)
+{
+    y_c2c_pipe<T, INV, SH>(in, in_pitch, out, out_pitch, ncols, nz, tw, dc_shift, skip);
+}
+
+// FP64 tiles (half width, 256 threads): three resident CTAs per SM, which
+// bounds the registers to 85 a thread
+template <bool INV, typename SH>
+__global__ void __launch_bounds__(SH::NT, 3) k_y_c2c_pipe64(const cx<double>* __restrict__ in, long in_pitch,
+                                                           cx<double>* __restrict__ out, long out_pitch, int ncols,
+                                                           int nz, const cx<double>* __restrict__ tw,
+                                                           const double* __restrict__ dc_shift,
+                                                           const int* __restrict__ skip)
+{
+    y_c2c_pipe<double, INV, SH>(in, in_pitch, out, out_pitch, ncols, nz, tw, dc_shift, skip);
+}
+
 // Tile shape of the pipelined y kernel.  FP64 tiles of 512-thread shapes
 // are halved (W/2 columns, 256 threads): two 32 KB buffers per CTA let three
-// CTAs share an SM, and 8 complex values per thread fit without spills.
+// CTAs share an SM, with 8 complex values per thread.
 template <typename T, typename SH>
 struct PipeShape {
     using type = SH;
@@ -251,7 +272,10 @@ template <typename T, bool INV, typename SH>
 cudaError_t launch_y_c2c_pipe(const cx<T>* in, long in_pitch, cx<T>* out, long out_pitch, int ncols, int nz,
                               const cx<T>* tw, const double* dc_shift, const int* skip_flag, cudaStream_t st)
 {
-    auto kern = k_y_c2c_pipe<T, INV, SH>;
+    auto kern = [] {
+        if constexpr (sizeof(T) == 8) return k_y_c2c_pipe64<INV, SH>;
+        else return k_y_c2c_pipe<T, INV, SH>;
+    }();
     const size_t smem = 2 * (size_t)SH::N * SH::W * sizeof(cx<T>);
     cudaError_t e = set_smem(kern, smem);
     if (e != cudaSuccess) return e;
