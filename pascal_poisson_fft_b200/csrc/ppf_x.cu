@@ -20,11 +20,10 @@ constexpr int MAXW = 128;  // widest tile of any shape (FP32, n = 32)
 // (R2C, complex rows of nx/2+1) or DCT-II (real rows of nx).
 // --------------------------------------------------------------------------
 template <typename T, bool DCT, bool RESID, typename SH>
-__global__ void __launch_bounds__(512) k_xfwd(const double* __restrict__ f, ResidIn rs, Geom g,
-                                               void* __restrict__ out_, long out_pitch, FftSched sch, int Wrt,
-                                               int lgWrt, const cx<T>* __restrict__ tw_half,
-                                               const cx<T>* __restrict__ tw_n, const cx<T>* __restrict__ tw_dct,
-                                               const int* __restrict__ skip)
+__device__ __forceinline__ void xfwd(const double* __restrict__ f, const ResidIn& rs, const Geom& g,
+                                     void* __restrict__ out_, long out_pitch, const FftSched& sch, int Wrt, int lgWrt,
+                                     const cx<T>* __restrict__ tw_half, const cx<T>* __restrict__ tw_n,
+                                     const cx<T>* __restrict__ tw_dct, const int* __restrict__ skip)
 {
     if (skip && *skip) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -179,18 +178,36 @@ __global__ void __launch_bounds__(512) k_xfwd(const double* __restrict__ f, Resi
     }
 }
 
+#define PPF_XFWD_PARAMS                                                                                      \
+    const double* __restrict__ f, ResidIn rs, Geom g, void* __restrict__ out_, long out_pitch, FftSched sch,    \
+        int Wrt, int lgWrt, const cx<T>* __restrict__ tw_half, const cx<T>* __restrict__ tw_n,                \
+        const cx<T>* __restrict__ tw_dct, const int* __restrict__ skip
+#define PPF_XFWD_ARGS f, rs, g, out_, out_pitch, sch, Wrt, lgWrt, tw_half, tw_n, tw_dct, skip
+
+template <typename T, bool DCT, bool RESID, typename SH>
+__global__ void __launch_bounds__(512) k_xfwd(PPF_XFWD_PARAMS)
+{
+    xfwd<T, DCT, RESID, SH>(PPF_XFWD_ARGS);
+}
+
+// FP64 compile-time tiles: five resident CTAs of SH::NT threads per SM
+template <bool DCT, typename SH, typename T = double>
+__global__ void __launch_bounds__(SH::NT, 5) k_xfwd64(PPF_XFWD_PARAMS)
+{
+    xfwd<T, DCT, false, SH>(PPF_XFWD_ARGS);
+}
+
 // --------------------------------------------------------------------------
 // x inverse: half spectrum (C2R) or DCT coefficients (inverse DCT) ->
 // interior of the ghosted FP64 output.  ACC: u <- (u - mean_prev) + du.
 // partials (optional): per-block [sum du^2, sum u^2, sum u].
 // --------------------------------------------------------------------------
 template <typename T, bool DCT, bool ACC, bool GHOST, typename SH>
-__global__ void __launch_bounds__(512) k_xinv(const void* __restrict__ in_, long in_pitch, double* __restrict__ P,
-                                               Geom g, double* __restrict__ partials,
-                                               const double* __restrict__ mean_prev, FftSched sch, int Wrt,
-                                               int lgWrt, const cx<T>* __restrict__ tw_half,
-                                               const cx<T>* __restrict__ tw_n, const cx<T>* __restrict__ tw_dct,
-                                               const int* __restrict__ skip)
+__device__ __forceinline__ void xinv(const void* __restrict__ in_, long in_pitch, double* __restrict__ P,
+                                     const Geom& g, double* __restrict__ partials,
+                                     const double* __restrict__ mean_prev, const FftSched& sch, int Wrt, int lgWrt,
+                                     const cx<T>* __restrict__ tw_half, const cx<T>* __restrict__ tw_n,
+                                     const cx<T>* __restrict__ tw_dct, const int* __restrict__ skip)
 {
     if (skip && *skip) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -384,6 +401,26 @@ __global__ void __launch_bounds__(512) k_xinv(const void* __restrict__ in_, long
     }
 }
 
+#define PPF_XINV_PARAMS                                                                                      \
+    const void* __restrict__ in_, long in_pitch, double* __restrict__ P, Geom g, double* __restrict__ partials, \
+        const double* __restrict__ mean_prev, FftSched sch, int Wrt, int lgWrt,                                \
+        const cx<T>* __restrict__ tw_half, const cx<T>* __restrict__ tw_n, const cx<T>* __restrict__ tw_dct,   \
+        const int* __restrict__ skip
+#define PPF_XINV_ARGS in_, in_pitch, P, g, partials, mean_prev, sch, Wrt, lgWrt, tw_half, tw_n, tw_dct, skip
+
+template <typename T, bool DCT, bool ACC, bool GHOST, typename SH>
+__global__ void __launch_bounds__(512) k_xinv(PPF_XINV_PARAMS)
+{
+    xinv<T, DCT, ACC, GHOST, SH>(PPF_XINV_ARGS);
+}
+
+// FP64 compile-time tiles: five resident CTAs of SH::NT threads per SM
+template <bool DCT, typename SH, typename T = double>
+__global__ void __launch_bounds__(SH::NT, 5) k_xinv64(PPF_XINV_PARAMS)
+{
+    xinv<T, DCT, false, false, SH>(PPF_XINV_ARGS);
+}
+
 // --------------------------------------------------------------------------
 // x inverse of FP32 spectra, periodic x, compile-time shapes: persistent
 // CTAs walk tiles of W lines; the next tile's half-spectrum rows are copied
@@ -556,6 +593,13 @@ cudaError_t launch_xfwd(bool dct, const double* f, const ResidIn* resid, const G
                                               skip_flag);
             err = cudaGetLastError();
         };
+        if constexpr (SH::CT && sizeof(T) == 8) {
+            if (!resid) {
+                if (dct) go(k_xfwd64<true, SH>);
+                else go(k_xfwd64<false, SH>);
+                return;
+            }
+        }
         if (dct) {
             if (resid) go(k_xfwd<T, true, true, SH>);
             else go(k_xfwd<T, true, false, SH>);
@@ -606,6 +650,13 @@ cudaError_t launch_xinv(bool dct, const void* in, long in_pitch, double* P, cons
                 if (!stencil_ghosts) pipe(k_xinv_pipe<T, false, false, SH>);
                 else if (accumulate) pipe(k_xinv_pipe<T, true, true, SH>);
                 else pipe(k_xinv_pipe<T, false, true, SH>);
+                return;
+            }
+        }
+        if constexpr (SH::CT && sizeof(T) == 8) {
+            if (!stencil_ghosts && !accumulate) {
+                if (dct) go(k_xinv64<true, SH>);
+                else go(k_xinv64<false, SH>);
                 return;
             }
         }
