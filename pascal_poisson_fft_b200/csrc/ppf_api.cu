@@ -111,7 +111,7 @@ struct ppf_plan {
     double* am = nullptr;
     double* ap = nullptr;
     double* scal = nullptr;    // [0] min dz^2, [3] last ||du||/||u||, [4] zero-mode shift, [5] mean of the iterate
-    int* flags = nullptr;      // [0] skip, [1] sweeps_done, [2] err
+    int* flags = nullptr;      // [0] skip, [1] sweeps_done, [2] err, [3] FP64 low-|k| systems of a mixed solve
     double* partials = nullptr;  // per-block sums of the x-inverse pass (mixed precision)
     long xinv_nblk = 0;
     double* ckpt = nullptr;      // Thomas checkpoints of the z solve
@@ -348,7 +348,31 @@ int run_pass(ppf_plan* p, const double* f, double* P, bool resid, bool accumulat
         rs.ix2 = 1.0 / (hx * hx);
         rs.iy2 = 1.0 / (hy * hy);
     }
+    ZSys z{};
+    z.mx = p->mx; z.my = p->my; z.pitch = p->b_pitch; z.plane = p->b_pitch * (long)p->my; z.nz = p->g.nz;
+    z.lamx = p->lamx; z.lamy = p->lamy; z.am = p->am; z.ap = p->ap; z.scale = p->scale;
+    z.lowk = (p->d.precision == PPF_FP64) ? 0.0 : p->d.lowk_threshold;
+    z.dzmin2 = p->scal;
+    z.dc_shift = p->scal + 4;
+    z.cyclic = p->g.pz;
+    z.ckpt = p->ckpt;
+    z.ckpt_f = (sizeof(T) == 4) ? tdma_z_ckpt_f32(p->ckpt, z.nz, z.plane, z.cyclic) : nullptr;
+    if (sizeof(T) == 4 && !z.cyclic) {
+        // the FP64 low-|k| systems: their list, and the table of their
+        // coefficient sweeps in the FP64 checkpoint region (unused here)
+        z.lowk_count = p->flags + 3;
+        z.lowk_list = tdma_z_lowk_list(p->ckpt, z.nz, z.plane, z.cyclic);
+        z.lowk_tab = p->ckpt;
+        z.lowk_cap = tdma_z_ckpt_doubles(z.nz, z.plane, z.cyclic, false);
+        z.lowk_build = !resid;
+    }
     cudaError_t e;
+    if (!resid && z.lowk_list) {
+        // the FP64 low-|k| set of this solve (flags[3], zeroed with the
+        // flags, counts it); the z solve of every pass uses it
+        e = launch_lowk_list(z, st);
+        if (e != cudaSuccess) return cuda_fail(e, "low-|k| list");
+    }
     e = launch_xfwd<T>(p->xdct, f, resid ? &rs : nullptr, p->g, p->A, p->a_pitch, p->sx, txh, txn, txd, skip, st);
     if (e != cudaSuccess) return cuda_fail(e, "x forward");
     mark(p, 1, st);
@@ -359,15 +383,6 @@ int run_pass(ppf_plan* p, const double* f, double* P, bool resid, bool accumulat
                        p->ycols, p->g, p->sy, tyn, tyd, skip, st);
     if (e != cudaSuccess) return cuda_fail(e, "y forward");
     mark(p, 2, st);
-    ZSys z{};
-    z.mx = p->mx; z.my = p->my; z.pitch = p->b_pitch; z.plane = p->b_pitch * (long)p->my; z.nz = p->g.nz;
-    z.lamx = p->lamx; z.lamy = p->lamy; z.am = p->am; z.ap = p->ap; z.scale = p->scale;
-    z.lowk = (p->d.precision == PPF_FP64) ? 0.0 : p->d.lowk_threshold;
-    z.dzmin2 = p->scal;
-    z.dc_shift = p->scal + 4;
-    z.cyclic = p->g.pz;
-    z.ckpt = p->ckpt;
-    z.ckpt_f = (sizeof(T) == 4) ? tdma_z_ckpt_f32(p->ckpt, z.nz, z.plane, z.cyclic) : nullptr;
     const ZStreams zs{ st, p->aux, p->ev_fork, p->ev_join };
     e = p->cplx ? launch_tdma_z<T, true>(p->B, z, skip, p->flags + 2, zs)
                 : launch_tdma_z<T, false>(p->B, z, skip, p->flags + 2, zs);

@@ -54,7 +54,17 @@ __device__ __forceinline__ int sidx(int n, int l, int W)
 
 // Asynchronous global -> shared copies (cp.async): one element per call,
 // completion tracked per thread by commit groups.
+__device__ __forceinline__ void cp_async_elem(float* dst, const float* src)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+}
 __device__ __forceinline__ void cp_async_elem(cx<float>* dst, const cx<float>* src)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_f64(double* dst, const double* src)
 {
     const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");

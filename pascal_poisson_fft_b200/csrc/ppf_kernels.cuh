@@ -71,12 +71,20 @@ struct ZSys {
     int cyclic;           // periodic z: the reference's cyclic Thomas sequence
     double* ckpt;         // Thomas checkpoints, tdma_z_ckpt_doubles(nz, plane, cyclic, fp32) doubles
     float* ckpt_f;        // FP32 checkpoints of the FP32 bulk kernel (tdma_z_ckpt_f32), or null
+    // FP32 storage, non-periodic z: the FP64 low-|k| systems
+    int* lowk_count;      // device count (zeroed before the list is built)
+    int* lowk_list;       // their indices (tdma_z_lowk_list), or null
+    double* lowk_tab;     // coefficient table of the first groups (lowk_cap doubles), or null
+    long lowk_cap;
+    int lowk_build;       // first pass of a solve: fill the table before the z solve
 };
 
 // doubles of checkpoint memory the z solve needs (fp32: FP32 spectral storage)
 long tdma_z_ckpt_doubles(int nz, long plane, int cyclic, bool fp32);
 // start of the FP32 checkpoint region inside a checkpoint buffer of FP32 storage
 float* tdma_z_ckpt_f32(double* ckpt, int nz, long plane, int cyclic);
+// the low-|k| system list inside a checkpoint buffer of FP32 storage
+int* tdma_z_lowk_list(double* ckpt, int nz, long plane, int cyclic);
 
 // streams of the z solve: the FP32 bulk runs on st; the FP64 low-|k|
 // systems run on aux (forked from and joined back to st through the two
@@ -89,6 +97,10 @@ struct ZStreams {
 
 template <typename T, bool CPLX>
 cudaError_t launch_tdma_z(void* data, const ZSys& z, const int* skip_flag, int* err_flag, const ZStreams& zs);
+
+// the low-|k| system list of a mixed or FP32 solve (z.lowk_list), once per
+// solve before its first z solve; a no-op where the list is not used
+cudaError_t launch_lowk_list(const ZSys& z, cudaStream_t st);
 
 cudaError_t launch_zcoef(const double* dx3, const double* dmx3, int nz, double* am, double* ap,
                          double* dzmin2, cudaStream_t st);

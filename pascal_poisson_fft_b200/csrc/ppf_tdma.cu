@@ -379,13 +379,20 @@ long tdma_z_ckpt_doubles(int nz, long plane, int cyclic, bool fp32)
     const int ch = Exact::CH < Fast::CH ? Exact::CH : Fast::CH;   // the finer chunking of the two paths
     const long nch = (m + ch - 1) / ch;
     const long dbl = nch * (cyclic ? 4 : 3) * plane;
-    // FP32 storage: FP32 checkpoints of the bulk kernel follow the FP64 ones
-    return fp32 ? dbl + (dbl + 1) / 2 : dbl;
+    // FP32 storage: FP32 checkpoints of the bulk kernel follow the FP64 ones,
+    // then the low-|k| list (at most plane system indices)
+    return fp32 ? dbl + (dbl + 1) / 2 + (plane + 2) / 2 + 1 : dbl;
 }
 
 float* tdma_z_ckpt_f32(double* ckpt, int nz, long plane, int cyclic)
 {
     return reinterpret_cast<float*>(ckpt + tdma_z_ckpt_doubles(nz, plane, cyclic, false));
+}
+
+int* tdma_z_lowk_list(double* ckpt, int nz, long plane, int cyclic)
+{
+    const long dbl = tdma_z_ckpt_doubles(nz, plane, cyclic, false);
+    return reinterpret_cast<int*>(ckpt + dbl + (dbl + 1) / 2);
 }
 
 namespace {
@@ -625,6 +632,313 @@ __global__ void __launch_bounds__(TPB) k_thomas_exact(void* __restrict__ data_, 
     if (bad && err) atomicOr(err, 1);
 }
 
+// Low-|k| systems of the mixed-precision z solve (lam * dz_min^2 < lowk, the
+// complement of k_thomas_fast's set): one thread per system, a warp ballot
+// and one atomic per warp append them to the list.  The order of the list
+// does not matter for the results (every system is solved on its own), so
+// no scan is needed.  Runs once per solve, after the z-coefficient kernel
+// (dz_min) and with the count zeroed.
+__global__ void __launch_bounds__(256) k_lowk_list(ZSys z)
+{
+    const long s = (long)blockIdx.x * 256 + threadIdx.x;
+    bool low = false;
+    if (s < z.plane) {
+        const int kx = (int)s % (int)z.pitch, ky = (int)s / (int)z.pitch;
+        low = kx < z.mx && ky < z.my && (z.lamx[kx] + z.lamy[ky]) * __ldg(z.dzmin2) < z.lowk;
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, low);
+    if (!m) return;
+    const int lane = threadIdx.x & 31;
+    int base = 0;
+    if (lane == 0) base = atomicAdd(z.lowk_count, __popc(m));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (low) z.lowk_list[base + __popc(m & ((1u << lane) - 1))] = (int)s;
+}
+
+// the list exists for FP32 storage with non-periodic z and 32-bit indices
+bool lowk_listed(const ZSys& z)
+{
+    return z.lowk_list && z.lowk_count && !z.cyclic && z.lowk > 0.0 && z.plane < (1L << 30);
+}
+
+constexpr int LK_NS = 8;   // ring slots of the low-|k| kernel, Exact::CH rows each
+
+template <bool CPLX>
+size_t lowk_smem(int nz)
+{
+    const size_t nch = (size_t)(nz + Exact::CH - 1) / Exact::CH;
+    return sizeof(double) * (3 * (size_t)nz + 96 * nch + 96 * Exact::CH) +
+           (sizeof(typename Elem<float, CPLX>::type) + sizeof(double)) * LK_NS * Exact::CH * 32;
+}
+
+// the level coefficients am, ap, -am - ap of the z operator into shared memory
+__device__ __forceinline__ void stage_levels(const ZSys& z, double* zl)
+{
+    const int nz = z.nz;
+    for (int k = threadIdx.x; k < nz; k += blockDim.x) {
+        const double am = z.am[k], ap = z.ap[k];
+        zl[k] = am;
+        zl[nz + k] = ap;
+        zl[2 * nz + k] = __dsub_rn(-am, ap);
+    }
+}
+
+// The coefficient half of the low-|k| Thomas sweep, which does not depend on
+// the right-hand side: c'_1 = c_1 / b_1 and, below the first row,
+// r_k = 1 / (b_k - a_k c'_{k-1}), c'_k = r_k c_k, with thomas_poisson<Exact>'s
+// operations.  Table entry k of a system holds r_k (c'_1 for the first row),
+// [group][row][lane], for the groups of 32 listed systems that fit in `cap`
+// doubles.  Once per solve: every pass of the solve has the same operator.
+__global__ void __launch_bounds__(32) k_lowk_table(ZSys z, const int* __restrict__ skip)
+{
+    if (skip && *skip) return;
+    using X = Exact;
+    extern __shared__ double zl[];
+    stage_levels(z, zl);
+    __syncwarp();
+    const int nz = z.nz, lane = threadIdx.x;
+    const int count = *z.lowk_count;
+    for (int g = blockIdx.x; g * 32 < count && (long)(g + 1) * 32 * nz <= z.lowk_cap; g += gridDim.x) {
+        const int idx = g * 32 + lane;
+        if (idx >= count) continue;
+        const int sys = z.lowk_list[idx];
+        const int kx = sys % (int)z.pitch, ky = sys / (int)z.pitch;
+        const double lx = z.lamx[kx], ly = z.lamy[ky];
+        const bool pin = (kx == 0 && ky == 0);
+        double* tab = z.lowk_tab + (size_t)g * nz * 32 + lane;
+        double cp = pin ? X::div(0.0, 1.0) : X::div(zl[nz], X::sub(X::sub(zl[2 * nz], lx), ly));
+        tab[0] = cp;
+#pragma unroll 4
+        for (int zr = 1; zr < nz; ++zr) {
+            const double b = X::sub(X::sub(zl[2 * nz + zr], lx), ly);
+            const double r = X::rcp(X::sub(b, X::mul(zl[zr], cp)));
+            cp = X::mul(r, zl[nz + zr]);
+            tab[(size_t)zr * 32] = r;
+        }
+    }
+}
+
+// One group of 32 listed systems (one per lane) of k_thomas_lowk.  TAB: r_k
+// and c'_1 come from the k_lowk_table entries, streamed through the ring
+// beside the rows, so the sweeps are multiply-subtract chains; otherwise the
+// reciprocals are formed here.  Either way the operations and their order
+// are thomas_poisson<float, Exact>'s.
+template <bool CPLX, bool TAB>
+__device__ __forceinline__ void lowk_group(void* data_, const ZSys& z, int g, int sys, const double* zl, double* ckp,
+                                           double* scr, typename Elem<float, CPLX>::type* ring, double* rring,
+                                           int* err)
+{
+    using E = typename Elem<float, CPLX>::type;
+    using X = Exact;
+    constexpr int C = Exact::CH;
+    const int nz = z.nz, nch = (nz + C - 1) / C, lane = threadIdx.x;
+    const long plane = z.plane;
+    const int kx = sys % (int)z.pitch, ky = sys / (int)z.pitch;
+    const double lx = z.lamx[kx], ly = z.lamy[ky];
+    const bool pin = (kx == 0 && ky == 0);
+    E* col = reinterpret_cast<E*>(data_) + sys;
+    const double* tab = TAB ? z.lowk_tab + (size_t)g * nz * 32 + lane : nullptr;
+    // chunk ch into its slot; one commit group per call, empty out of range
+    auto issue = [&](int ch) {
+        if (ch >= 0 && ch < nch) {
+            const size_t so = (size_t)(ch % LK_NS) * C * 32 + lane;
+            const int nq = min(C, nz - ch * C);
+            for (int q = 0; q < nq; ++q) {
+                cp_async_elem(ring + so + q * 32, col + (long)(ch * C + q) * plane);
+                if (TAB) cp_async_f64(rring + so + q * 32, tab + (size_t)(ch * C + q) * 32);
+            }
+        }
+        cp_async_commit();
+    };
+    const double b0 = pin ? 1.0 : X::sub(X::sub(zl[2 * nz], lx), ly);
+    // the first row: d'_1 = d_1 / b_1 (pinned: a, b, c, d = 0, 1, 0, 0)
+    auto first = [&](const E* v, const double* rv, double& cp, double& dr, double& di) {
+        double vr, vi;
+        ld_cv<float, double>(v, vr, vi);
+        if (pin) { vr = 0.0; vi = 0.0; }
+        if (TAB) {
+            dr = X::div(vr, b0);
+            if (CPLX) di = X::div(vi, b0);
+            cp = *rv;
+        } else {
+            fwd_row<Exact, CPLX>(true, 0.0, b0, pin ? 0.0 : zl[nz], vr, vi, cp, dr, di);
+        }
+    };
+    // a row below the first, b = ((-am - ap) - lx) - ly
+    auto step = [&](int zr, const E* v, const double* rv, double& cp, double& dr, double& di) {
+        double vr, vi;
+        ld_cv<float, double>(v, vr, vi);
+        const double a = zl[zr];
+        if (TAB) {
+            const double r = *rv;
+            dr = X::mul(r, X::sub(vr, X::mul(a, dr)));
+            if (CPLX) di = X::mul(r, X::sub(vi, X::mul(a, di)));
+            cp = X::mul(r, zl[nz + zr]);
+        } else {
+            const double b = X::sub(X::sub(zl[2 * nz + zr], lx), ly);
+            fwd_row<Exact, CPLX>(false, a, b, zl[nz + zr], vr, vi, cp, dr, di);
+        }
+    };
+    for (int c = 0; c < LK_NS - 1; ++c) issue(c);
+    double cp = 0, dr = 0, di = 0;
+    for (int ch = 0; ch < nch; ++ch) {
+        cp_async_wait<LK_NS - 2>();          // chunk ch has landed
+        issue(ch + LK_NS - 1);               // into the slot chunk ch - 1 left
+        const size_t so = (size_t)(ch % LK_NS) * C * 32 + lane;
+        const int z0 = ch * C, nq = min(C, nz - z0);
+        if (TAB && ch > 0 && nq == C) {
+            // a full chunk: the rows and table entries into registers, then
+            // the chain (multiply, subtract, multiply per row)
+            double vr[C], vi[C], rr[C];
+#pragma unroll
+            for (int q = 0; q < C; ++q) {
+                ld_cv<float, double>(ring + so + q * 32, vr[q], vi[q]);
+                rr[q] = rring[so + q * 32];
+            }
+#pragma unroll
+            for (int q = 0; q < C; ++q) {
+                const double a = zl[z0 + q];
+                dr = X::mul(rr[q], X::sub(vr[q], X::mul(a, dr)));
+                if (CPLX) di = X::mul(rr[q], X::sub(vi[q], X::mul(a, di)));
+            }
+        } else {
+            int q = 0;
+            if (ch == 0) { first(ring + so, rring + so, cp, dr, di); q = 1; }
+#pragma unroll 1
+            for (; q < nq; ++q) step(z0 + q, ring + so + q * 32, rring + so + q * 32, cp, dr, di);
+        }
+        double* c3 = ckp + (size_t)ch * 96 + lane;
+        c3[0] = cp;
+        c3[32] = dr;
+        c3[64] = di;
+    }
+    double xr = 0, xi = 0, zsum = 0.0;
+    bool bad = false;
+    for (int ch = nch - 1; ch >= 0; --ch) {
+        cp_async_wait<LK_NS - 1>();          // the top LK_NS chunks are resident since the forward sweep
+        const size_t so = (size_t)(ch % LK_NS) * C * 32 + lane;
+        const int z0 = ch * C, nq = min(C, nz - z0);
+        if (TAB && ch > 0 && nq == C) {
+            // a full chunk in registers: recompute d' from the checkpoint,
+            // c' = r c, then substitute
+            double vr[C], vi[C], rr[C];
+#pragma unroll
+            for (int q = 0; q < C; ++q) {
+                ld_cv<float, double>(ring + so + q * 32, vr[q], vi[q]);
+                rr[q] = rring[so + q * 32];
+            }
+            const double* c3 = ckp + (size_t)(ch - 1) * 96 + lane;
+            double pdr = c3[32], pdi = c3[64];
+#pragma unroll
+            for (int q = 0; q < C; ++q) {
+                const double a = zl[z0 + q];
+                pdr = X::mul(rr[q], X::sub(vr[q], X::mul(a, pdr)));
+                if (CPLX) pdi = X::mul(rr[q], X::sub(vi[q], X::mul(a, pdi)));
+                vr[q] = pdr;
+                vi[q] = pdi;
+                rr[q] = X::mul(rr[q], zl[nz + z0 + q]);
+            }
+            issue(ch - LK_NS);               // the slot just consumed
+#pragma unroll
+            for (int q = C - 1; q >= 0; --q) {
+                const int zr = z0 + q;
+                if (zr == nz - 1) {
+                    xr = vr[q];
+                    xi = vi[q];
+                } else {
+                    xr = X::sub(vr[q], X::mul(rr[q], xr));
+                    if (CPLX) xi = X::sub(vi[q], X::mul(rr[q], xi));
+                }
+                const double sr = xr * z.scale, si = xi * z.scale;
+                zsum += sr;
+                if (!isfinite(sr) || !isfinite(si)) bad = true;
+                st_elem<float>(col + (long)zr * plane, sr, si);
+            }
+            continue;
+        }
+        double pcp = 0, pdr = 0, pdi = 0;
+        int q = 0;
+        if (ch > 0) {
+            const double* c3 = ckp + (size_t)(ch - 1) * 96 + lane;
+            pcp = c3[0];
+            pdr = c3[32];
+            pdi = c3[64];
+        } else {
+            first(ring + so, rring + so, pcp, pdr, pdi);
+            scr[lane] = pcp; scr[32 + lane] = pdr; scr[64 + lane] = pdi;
+            q = 1;
+        }
+#pragma unroll 1
+        for (; q < nq; ++q) {
+            step(z0 + q, ring + so + q * 32, rring + so + q * 32, pcp, pdr, pdi);
+            double* r3 = scr + q * 96 + lane;
+            r3[0] = pcp; r3[32] = pdr; r3[64] = pdi;
+        }
+        issue(ch - LK_NS);                   // the slot just consumed
+        for (q = nq - 1; q >= 0; --q) {
+            const int zr = z0 + q;
+            const double* r3 = scr + q * 96 + lane;
+            if (zr == nz - 1) {
+                xr = r3[32];
+                xi = r3[64];
+            } else {
+                xr = X::sub(r3[32], X::mul(r3[0], xr));
+                if (CPLX) xi = X::sub(r3[64], X::mul(r3[0], xi));
+            }
+            const double sr = xr * z.scale, si = xi * z.scale;
+            zsum += sr;
+            if (!isfinite(sr) || !isfinite(si)) bad = true;
+            st_elem<float>(col + (long)zr * plane, sr, si);
+        }
+    }
+    cp_async_wait<0>();
+    if (pin && z.dc_shift) *z.dc_shift = zsum / (double)nz;
+    if (bad && err) atomicOr(err, 1);
+}
+
+// FP64 z solve of the listed low-|k| systems with FP32 spectral storage:
+// thomas_poisson<float, Exact> operation for operation (same results, bit
+// for bit), organised for latency.  Persistent one-warp blocks take 32
+// systems of the list at a time, one lane per system.  Every lane streams
+// its column (and the group's table entries) through its own ring of LK_NS
+// chunks in shared memory with cp.async, so up to LK_NS - 1 chunks of rows
+// are in flight while it eliminates: the sweeps are bound by their FP64
+// dependency chains, not by one HBM round trip per chunk under the
+// concurrent bulk kernel's load.  The first row (the only division) is
+// peeled and the row loops are not unrolled, so one warp per SM runs a short
+// instruction stream.  The forward checkpoints, the level coefficients and
+// the recomputed chunk of the backward sweep stay in shared memory; the
+// backward sweep finds the top LK_NS chunks still in the ring and refills
+// every slot it empties with the chunk LK_NS below.  A lane only reads what
+// it wrote or copied itself, so no barrier is needed after the staging.
+template <bool CPLX>
+__global__ void __launch_bounds__(32) k_thomas_lowk(void* __restrict__ data_, ZSys z, const int* __restrict__ skip,
+                                                    int* __restrict__ err)
+{
+    if (skip && *skip) return;
+    using E = typename Elem<float, CPLX>::type;
+    constexpr int C = Exact::CH;
+    const int nz = z.nz, nch = (nz + C - 1) / C;
+    extern __shared__ double lk[];
+    double* zl = lk;                                              // am[nz], ap[nz], -am - ap[nz]
+    double* ckp = zl + 3 * nz;                                    // [chunk][3][32]
+    double* scr = ckp + (size_t)nch * 96;                         // [C][3][32] recomputed chunk
+    double* rring = scr + 96 * C;                                 // [LK_NS][C][32] table entries
+    E* ring = reinterpret_cast<E*>(rring + LK_NS * C * 32);       // [LK_NS][C][32] rows
+    stage_levels(z, zl);
+    __syncwarp();
+    const int count = *z.lowk_count;
+    for (int g = blockIdx.x; g * 32 < count; g += gridDim.x) {
+        const int idx = g * 32 + threadIdx.x;
+        if (idx >= count) continue;
+        const int sys = z.lowk_list[idx];
+        if (z.lowk_tab && (long)(g + 1) * 32 * nz <= z.lowk_cap)
+            lowk_group<CPLX, true>(data_, z, g, sys, zl, ckp, scr, ring, rring, err);
+        else
+            lowk_group<CPLX, false>(data_, z, g, sys, zl, ckp, scr, ring, rring, err);
+    }
+}
+
 template <bool CPLX, bool CYC>
 cudaError_t launch_z(double*, const ZSys& z, void* data, const int* skip, int* err, const ZStreams& zs)
 {
@@ -647,7 +961,25 @@ cudaError_t launch_z(float*, const ZSys& z, void* data, const int* skip, int* er
         if (e != cudaSuccess) return e;
         lo = zs.aux;
     }
-    k_thomas_z<float, Exact, CPLX, 2, CYC><<<grid, TPB, 0, lo>>>(data, z, skip, err);
+    const size_t lsm = lowk_smem<CPLX>(z.nz);
+    if (!CYC && lowk_listed(z) && lsm <= 160 * 1024) {
+        // persistent one-warp blocks (one per SM) over the list; the first
+        // pass of a solve fills the coefficient table before
+        int dev = 0, sms = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(k_thomas_lowk<CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsm);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_lowk_table, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(3 * sizeof(double) * z.nz));
+        if (e != cudaSuccess) return e;
+        const long groups = (z.plane + 31) / 32;
+        const unsigned lg = (unsigned)(groups < sms ? groups : sms);
+        if (z.lowk_tab && z.lowk_build)
+            k_lowk_table<<<lg, 32, 3 * sizeof(double) * z.nz, lo>>>(z, skip);
+        k_thomas_lowk<CPLX><<<lg, 32, lsm, lo>>>(data, z, skip, err);
+    } else {
+        k_thomas_z<float, Exact, CPLX, 2, CYC><<<grid, TPB, 0, lo>>>(data, z, skip, err);
+    }
     if (CYC || !z.ckpt_f)
         k_thomas_z<float, Fast, CPLX, 1, CYC><<<grid, TPB, 0, zs.st>>>(data, z, skip, err);
     else
@@ -660,6 +992,13 @@ cudaError_t launch_z(float*, const ZSys& z, void* data, const int* skip, int* er
     return cudaGetLastError();
 }
 }  // namespace
+
+cudaError_t launch_lowk_list(const ZSys& z, cudaStream_t st)
+{
+    if (!lowk_listed(z)) return cudaSuccess;
+    k_lowk_list<<<(unsigned)((z.plane + 255) / 256), 256, 0, st>>>(z);
+    return cudaGetLastError();
+}
 
 template <typename T, bool CPLX>
 cudaError_t launch_tdma_z(void* data, const ZSys& z, const int* skip_flag, int* err_flag, const ZStreams& zs)

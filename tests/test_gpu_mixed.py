@@ -73,3 +73,23 @@ def test_fp32_768x768x384_radix3():
     P64 = gpu_solve(p)
     assert rel_l2(gpu_solve(p, precision=PPF_MIXED, max_sweeps=3), P64) < TOL_MIXED
     assert rel_l2(gpu_solve(p, precision=PPF_FP32), P64) < 2e-4
+
+
+# The FP64 systems of the mixed path (lam * dz_min^2 < lowk_threshold) run in
+# their own latency-bound kernel over a compacted list.  A threshold above
+# every eigenvalue sends all systems there: several 32-system groups per
+# persistent block, real (DCT x and y) and complex storage, columns shorter
+# than its prefetch ring and lengths that are no multiple of its chunk.
+@pytest.mark.parametrize("shape,pbc,lowk", [
+    ((128, 96, 40), (1, 1, 0), 1e12),
+    ((48, 40, 37), (0, 0, 0), 1e12),
+    ((64, 32, 21), (0, 1, 0), 1e12),
+    ((32, 48, 200), (1, 0, 0), 1e-3),
+])
+def test_mixed_lowk_systems(shape, pbc, lowk):
+    rng = np.random.default_rng(21)
+    p = W.random_problem(rng, *shape, pbc, beta=1.5)
+    ref = oracle_solve(p)
+    P = gpu_solve(p, precision=PPF_MIXED, max_sweeps=3, lowk_threshold=lowk)
+    assert rel_l2(P, ref) < TOL_MIXED
+    assert rel_l2(gpu_solve(p, precision=PPF_FP32, lowk_threshold=lowk), ref) < TOL_FP32
