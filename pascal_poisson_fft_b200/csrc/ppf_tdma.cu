@@ -400,10 +400,16 @@ namespace {
 // lowk, non-periodic z).  The same Thomas sweep as thomas_poisson<Fast>,
 // with the level coefficients (am, ap, -am-ap) staged once per CTA in shared
 // memory (b = -am-ap - lam, a single rounding more than the FP64 order,
-// which the refinement absorbs), FP32 checkpoints in their own region, and
-// the next chunk's rows loaded while the current chunk is eliminated.
+// which the refinement absorbs) and FP32 checkpoints in their own region.
+// Kept lean because the kernel is close to issue-bound: the next chunk's
+// rows (and, backward, the next checkpoint) are loaded while the current
+// chunk is eliminated; full chunks run without per-row bounds tests, the
+// first row is peeled; row addresses are 32-bit row x plane products on the
+// column pointer; the back substitution starts from x = 0 above the top row
+// (x_top = d'_top - c'_top * 0 = d'_top exactly), and non-finite results
+// are detected once, on a running sum of the outputs.
 template <bool CPLX>
-__global__ void __launch_bounds__(TPB) k_thomas_fast(void* __restrict__ data_, ZSys z, const int* __restrict__ skip,
+__global__ void __launch_bounds__(TPB, CPLX ? 7 : 6) k_thomas_fast(void* __restrict__ data_, ZSys z, const int* __restrict__ skip,
                                                      int* __restrict__ err)
 {
     if (skip && *skip) return;
@@ -421,85 +427,124 @@ __global__ void __launch_bounds__(TPB) k_thomas_fast(void* __restrict__ data_, Z
     if (lam * __ldg(z.dzmin2) < z.lowk) return;  // solved in FP64 (includes the pinned zero mode)
     const float lamf = (float)lam, sc = (float)z.scale;
     const int nz = z.nz;
-    const long plane = z.plane;
+    const unsigned pl = (unsigned)z.plane;
     constexpr int C = Fast::CH;
     const int nch = (nz + C - 1) / C;
     E* col = reinterpret_cast<E*>(data_) + sys;
-    float* ck = z.ckpt_f + sys;
+    const float* ckr = z.ckpt_f + sys;
+    float* ckw = z.ckpt_f + sys;
+    auto row = [&](int zr) { return col + (size_t)(unsigned)zr * pl; };
     float nr[C], ni[C];
     auto load = [&](int z0) {
+        if (z0 + C <= nz) {
 #pragma unroll
-        for (int q = 0; q < C; ++q) {
-            nr[q] = 0.f;
-            ni[q] = 0.f;
-            if (z0 + q < nz) ld_cv<float, float>(col + (long)(z0 + q) * plane, nr[q], ni[q]);
+            for (int q = 0; q < C; ++q) ld_cv<float, float>(row(z0 + q), nr[q], ni[q]);
+        } else {
+#pragma unroll
+            for (int q = 0; q < C; ++q) {
+                nr[q] = 0.f;
+                ni[q] = 0.f;
+                if (z0 + q < nz) ld_cv<float, float>(row(z0 + q), nr[q], ni[q]);
+            }
+        }
+    };
+    // rows [q0, q1) of a chunk from state (cp, dr, di); keep: c', d' per row
+    auto elim = [&](int z0, float* vr, float* vi, float* cs, float& cp, float& dr, float& di) {
+        if (z0 == 0) {
+            const float4 l0 = zlev[0];
+            fwd_row<Fast, CPLX>(true, l0.x, l0.z - lamf, l0.y, vr[0], vi[0], cp, dr, di);
+            cs[0] = cp; vr[0] = dr; vi[0] = di;
+#pragma unroll
+            for (int q = 1; q < C; ++q) {
+                if (q < nz) {
+                    const float4 lv = zlev[q];
+                    fwd_row<Fast, CPLX>(false, lv.x, lv.z - lamf, lv.y, vr[q], vi[q], cp, dr, di);
+                }
+                cs[q] = cp; vr[q] = dr; vi[q] = di;
+            }
+        } else if (z0 + C <= nz) {
+#pragma unroll
+            for (int q = 0; q < C; ++q) {
+                const float4 lv = zlev[z0 + q];
+                fwd_row<Fast, CPLX>(false, lv.x, lv.z - lamf, lv.y, vr[q], vi[q], cp, dr, di);
+                cs[q] = cp; vr[q] = dr; vi[q] = di;
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < C; ++q) {
+                if (z0 + q < nz) {
+                    const float4 lv = zlev[z0 + q];
+                    fwd_row<Fast, CPLX>(false, lv.x, lv.z - lamf, lv.y, vr[q], vi[q], cp, dr, di);
+                }
+                cs[q] = cp; vr[q] = dr; vi[q] = di;
+            }
         }
     };
     load(0);
     float cp = 0.f, dr = 0.f, di = 0.f;
     for (int ch = 0; ch < nch; ++ch) {
-        float vr[C], vi[C];
+        float vr[C], vi[C], cs[C];
 #pragma unroll
         for (int q = 0; q < C; ++q) { vr[q] = nr[q]; vi[q] = ni[q]; }
         if (ch + 1 < nch) load((ch + 1) * C);
-        const int z0 = ch * C;
-#pragma unroll
-        for (int q = 0; q < C; ++q) {
-            const int zr = z0 + q;
-            if (zr < nz) {
-                const float4 lv = zlev[zr];
-                fwd_row<Fast, CPLX>(zr == 0, lv.x, lv.z - lamf, lv.y, vr[q], vi[q], cp, dr, di);
-            }
-        }
-        float* c3 = ck + (long)(3 * ch) * plane;
+        elim(ch * C, vr, vi, cs, cp, dr, di);
+        float* c3 = ckw + (size_t)(unsigned)(3 * ch) * pl;
         c3[0] = cp;
-        c3[plane] = dr;
-        if (CPLX) c3[2 * plane] = di;
+        c3[pl] = dr;
+        if (CPLX) c3[(size_t)2 * pl] = di;
     }
-    float xr = 0.f, xi = 0.f;
-    bool bad = false;
+    float xr = 0.f, xi = 0.f, fsum = 0.f;
     load((nch - 1) * C);
+    float kc = 0.f, kr = 0.f, ki = 0.f;           // checkpoint ending chunk ch - 1
+    if (nch > 1) {
+        const float* c3 = ckr + (size_t)(unsigned)(3 * (nch - 2)) * pl;
+        kc = c3[0];
+        kr = c3[pl];
+        if (CPLX) ki = c3[(size_t)2 * pl];
+    }
     for (int ch = nch - 1; ch >= 0; --ch) {
-        float vr[C], vi[C], c_[C];
+        float vr[C], vi[C], cs[C];
 #pragma unroll
         for (int q = 0; q < C; ++q) { vr[q] = nr[q]; vi[q] = ni[q]; }
-        float pcp = 0.f, pdr = 0.f, pdi = 0.f;
+        float pcp = kc, pdr = kr, pdi = ki;
         if (ch > 0) {
-            const float* c3 = ck + (long)(3 * (ch - 1)) * plane;
-            pcp = c3[0];
-            pdr = c3[plane];
-            if (CPLX) pdi = c3[2 * plane];
             load((ch - 1) * C);
+            if (ch > 1) {
+                const float* c3 = ckr + (size_t)(unsigned)(3 * (ch - 2)) * pl;
+                kc = c3[0];
+                kr = c3[pl];
+                if (CPLX) ki = c3[(size_t)2 * pl];
+            } else {
+                kc = 0.f; kr = 0.f; ki = 0.f;
+            }
         }
         const int z0 = ch * C;
+        elim(z0, vr, vi, cs, pcp, pdr, pdi);
+        if (z0 + C <= nz) {
 #pragma unroll
-        for (int q = 0; q < C; ++q) {
-            const int zr = z0 + q;
-            if (zr < nz) {
-                const float4 lv = zlev[zr];
-                fwd_row<Fast, CPLX>(zr == 0, lv.x, lv.z - lamf, lv.y, vr[q], vi[q], pcp, pdr, pdi);
-            }
-            c_[q] = pcp; vr[q] = pdr; vi[q] = pdi;
-        }
-#pragma unroll
-        for (int q = C - 1; q >= 0; --q) {
-            const int zr = z0 + q;
-            if (zr < nz) {
-                if (zr == nz - 1) {
-                    xr = vr[q];
-                    xi = vi[q];
-                } else {
-                    xr = vr[q] - c_[q] * xr;
-                    if (CPLX) xi = vi[q] - c_[q] * xi;
-                }
-                if (!isfinite(xr) || !isfinite(xi)) bad = true;
-                E* o = col + (long)zr * plane;
+            for (int q = C - 1; q >= 0; --q) {
+                xr = vr[q] - cs[q] * xr;
+                if (CPLX) xi = vi[q] - cs[q] * xi;
+                fsum += xr + xi;
+                E* o = row(z0 + q);
                 if constexpr (CPLX) *o = mk<float>(xr * sc, xi * sc);
                 else *o = xr * sc;
             }
+        } else {
+#pragma unroll
+            for (int q = C - 1; q >= 0; --q) {
+                if (z0 + q < nz) {
+                    xr = vr[q] - cs[q] * xr;
+                    if (CPLX) xi = vi[q] - cs[q] * xi;
+                    fsum += xr + xi;
+                    E* o = row(z0 + q);
+                    if constexpr (CPLX) *o = mk<float>(xr * sc, xi * sc);
+                    else *o = xr * sc;
+                }
+            }
         }
     }
-    if (bad && err) atomicOr(err, 1);
+    if (!isfinite(fsum) && err) atomicOr(err, 1);
 }
 
 
@@ -980,7 +1025,7 @@ cudaError_t launch_z(float*, const ZSys& z, void* data, const int* skip, int* er
     } else {
         k_thomas_z<float, Exact, CPLX, 2, CYC><<<grid, TPB, 0, lo>>>(data, z, skip, err);
     }
-    if (CYC || !z.ckpt_f)
+    if (CYC || !z.ckpt_f || z.plane >= (1L << 31) / 4)
         k_thomas_z<float, Fast, CPLX, 1, CYC><<<grid, TPB, 0, zs.st>>>(data, z, skip, err);
     else
         k_thomas_fast<CPLX><<<grid, TPB, sizeof(float4) * z.nz, zs.st>>>(data, z, skip, err);
