@@ -130,17 +130,29 @@ def measured_hbm_peak():
 
 
 def stage_bytes(p, prec_bytes, sweeps):
-    """Algorithmic bytes per stage, summed over one solve."""
+    """Algorithmic bytes per stage, summed over one solve (periodic x and y).
+
+    Every pass reads and writes one spectral field per y and z stage; the x
+    forward reads f (FP64) and writes the spectrum, the x inverse reads the
+    spectrum and writes the iterate.  With refinement sweeps the first
+    iterate is an FP32 ghosted field (4 bytes a cell, written by the first
+    pass, read by the first sweep's residual and accumulate); later sweeps
+    read and write the FP64 iterate (8 bytes a cell)."""
     n1, n2, n3 = p.n1m, p.n2m, p.n3m
     N = n1 * n2 * n3
-    spec = (n1 // 2 + 1) * n2 * n3 * 2 * prec_bytes  # one half-spectrum field (periodic x,y)
+    spec = (n1 // 2 + 1) * n2 * n3 * 2 * prec_bytes  # one half-spectrum field
     runs = 1 + sweeps
+    if sweeps == 0 or prec_bytes == 8:
+        u_read, u_rw = 0, 8 * N
+    else:
+        u_read = 4 * N + (sweeps - 1) * 8 * N           # residual reads of the iterate
+        u_rw = 4 * N + (4 * N + 8 * N) + (sweeps - 1) * 16 * N   # x-inverse writes + accumulate reads
     return {
-        "x-forward": runs * (8 * N + spec) + sweeps * 8 * N,
+        "x-forward": runs * (8 * N + spec) + u_read,
         "y-forward": runs * 2 * spec,
         "tdma-z": runs * 2 * spec,
         "y-inverse": runs * 2 * spec,
-        "x-inverse": runs * (spec + 8 * N) + sweeps * 8 * N,
+        "x-inverse": runs * spec + u_rw,
     }
 
 

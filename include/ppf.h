@@ -150,7 +150,10 @@ PPF_API int ppf_last_sweeps(ppf_plan *plan, int *sweeps, double *last_rel_update
 PPF_API int ppf_stage_timing(ppf_plan *plan, int enable);
 PPF_API int ppf_stage_times(ppf_plan *plan, double *ms, int *launches);
 
-/* Bytes of device work memory held by the plan. */
+/* Bytes of device work memory held by the plan for its solves: spectral
+ * buffers, z-solve checkpoints, and for a mixed-precision plan its partial
+ * sums and, when it refines (max_sweeps > 0), one FP32 ghosted field that
+ * holds the first iterate. */
 PPF_API int ppf_plan_workspace_bytes(const ppf_plan *plan, long long *bytes);
 
 /* Batched tridiagonal solves on device arrays, system index fastest:

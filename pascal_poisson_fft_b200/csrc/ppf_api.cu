@@ -116,7 +116,8 @@ struct ppf_plan {
     long xinv_nblk = 0;
     double* ckpt = nullptr;      // Thomas checkpoints of the z solve
     long ckpt_doubles = 0;
-    bool own_work = true;        // A, B, ckpt, partials belong to the plan (not to a batch)
+    float* U = nullptr;          // FP32 first iterate of a refining mixed solve (ghosted layout)
+    bool own_work = true;        // A, B, ckpt, partials, U belong to the plan (not to a batch)
     // auxiliary stream of the FP64 low-|k| z solves of the mixed and FP32 paths
     cudaStream_t aux = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
@@ -193,7 +194,7 @@ void free_plan(ppf_plan* p)
     if (p->ev_fork) cudaEventDestroy(p->ev_fork);
     if (p->ev_join) cudaEventDestroy(p->ev_join);
     if (p->own_work) {
-        void* work[] = { p->A, p->B, p->partials, p->ckpt };
+        void* work[] = { p->A, p->B, p->partials, p->ckpt, p->U };
         for (void* q : work)
             if (q) cudaFree(q);
     }
@@ -311,7 +312,15 @@ long partials_doubles(const ppf_plan* p)
     return (p->d.precision == PPF_MIXED) ? 3 * xinv_blocks<float>(p->g, p->sx) : 0;
 }
 
-// the plan's own work memory: spectral buffers, Thomas checkpoints, partials
+// the FP32 first iterate of a mixed solve that refines: ghosted, like P
+size_t u_bytes(const ppf_plan* p)
+{
+    if (p->d.precision != PPF_MIXED || p->d.max_sweeps == 0) return 0;
+    return sizeof(float) * (size_t)(p->g.nx + 2) * (p->g.ny + 2) * (p->g.nz + 2);
+}
+
+// the plan's own work memory: spectral buffers, Thomas checkpoints,
+// partials, the FP32 first iterate
 int plan_alloc_work(ppf_plan* p)
 {
     p->own_work = true;
@@ -326,12 +335,21 @@ int plan_alloc_work(ppf_plan* p)
         p->xinv_nblk = np / 3;
         PPF_CK(cudaMalloc(&p->partials, sizeof(double) * np));
     }
+    const size_t ub = u_bytes(p);
+    if (ub && cudaMalloc(&p->U, ub) != cudaSuccess) {
+        cudaGetLastError();
+        p->U = nullptr;
+        return fail(PPF_ERR_NOMEM, "cannot allocate %.1f MB for the FP32 first iterate", ub / 1048576.0);
+    }
     return PPF_OK;
 }
 
+// One pass of transforms and z solves.  uk (UKind): where the x inverse
+// puts the iterate (U_WRITE: the FP32 field p->U) and, with resid, where the
+// residual and the accumulate read it (U_ACC: from p->U).
 template <typename T>
 int run_pass(ppf_plan* p, const double* f, double* P, bool resid, bool accumulate, const int* skip,
-             cudaStream_t st)
+             cudaStream_t st, int uk = U_P)
 {
     const cx<T>* tw = reinterpret_cast<const cx<T>*>(p->tw);
     const cx<T>* txh = tw + p->tw_off[0];
@@ -342,6 +360,7 @@ int run_pass(ppf_plan* p, const double* f, double* P, bool resid, bool accumulat
     ResidIn rs{};
     if (resid) {
         rs.P = P;
+        rs.U = (uk == U_ACC) ? p->U : nullptr;
         rs.am = p->am;
         rs.ap = p->ap;
         const double hx = p->d.L1 / p->g.nx, hy = p->d.L2 / p->g.ny;
@@ -394,8 +413,8 @@ int run_pass(ppf_plan* p, const double* f, double* P, bool resid, bool accumulat
     mark(p, 4, st);
     // the mixed path keeps the stencil's ghost cells current for its residual
     long nblk = 0;
-    e = launch_xinv<T>(p->xdct, p->A, p->a_pitch, P, p->g, accumulate, p->d.precision == PPF_MIXED, p->partials,
-                       p->scal + 5, p->sx, txh, txn, txd, skip, st, &nblk);
+    e = launch_xinv<T>(p->xdct, p->A, p->a_pitch, P, p->U, uk, p->g, accumulate, p->d.precision == PPF_MIXED,
+                       p->partials, p->scal + 5, p->sx, txh, txn, txd, skip, st, &nblk);
     if (p->partials) p->xinv_nblk = nblk;  // the refinement gate reduces these blocks' partial sums
     if (e != cudaSuccess) return cuda_fail(e, "x inverse");
     mark(p, 5, st);
@@ -420,7 +439,10 @@ int solve_impl(ppf_plan* p, const double* f, double* P, const double* dmx1, cons
     if (p->elem == 8) {
         rc = run_pass<double>(p, f, P, false, false, nullptr, st);
     } else {
-        rc = run_pass<float>(p, f, P, false, false, nullptr, st);
+        // a refining mixed solve keeps its first iterate (FP32 values) in U;
+        // the first sweep reads it from there and writes P
+        const bool u32 = p->d.precision == PPF_MIXED && p->d.max_sweeps > 0 && p->U;
+        rc = run_pass<float>(p, f, P, false, false, nullptr, st, u32 ? U_WRITE : U_P);
         if (rc == PPF_OK && p->d.precision == PPF_MIXED) {
             const double ncell = (double)p->g.nx * p->g.ny * p->g.nz;
             e = launch_sweep_gate(p->partials, p->xinv_nblk, ncell, p->scal + 5, p->flags, p->flags + 1,
@@ -428,7 +450,7 @@ int solve_impl(ppf_plan* p, const double* f, double* P, const double* dmx1, cons
             if (e != cudaSuccess) return cuda_fail(e, "sweep gate");
             mark(p, 6, st);
             for (int s = 0; s < p->d.max_sweeps && rc == PPF_OK; ++s) {
-                rc = run_pass<float>(p, f, P, true, true, p->flags, st);
+                rc = run_pass<float>(p, f, P, true, true, p->flags, st, (u32 && s == 0) ? U_ACC : U_P);
                 if (rc != PPF_OK) break;
                 e = launch_sweep_gate(p->partials, p->xinv_nblk, ncell, p->scal + 5, p->flags, p->flags + 1,
                                       p->scal + 3, p->d.sweep_tol, 0, st);
@@ -603,7 +625,10 @@ int ppf_stage_times(ppf_plan* plan, double* ms, int* launches)
 int ppf_plan_workspace_bytes(const ppf_plan* plan, long long* bytes)
 {
     if (!plan || !bytes) return fail(PPF_ERR_INVALID, "null argument");
-    *bytes = (long long)(plan->a_bytes + plan->b_bytes);
+    // spectral buffers, z-solve checkpoints (and low-|k| list), partial sums,
+    // the FP32 first iterate of a refining mixed solve
+    *bytes = (long long)(plan->a_bytes + plan->b_bytes + sizeof(double) * plan->ckpt_doubles +
+                         sizeof(double) * partials_doubles(plan) + u_bytes(plan));
     return PPF_OK;
 }
 
@@ -830,7 +855,7 @@ int ppf_slab_inverse(ppf_plan* plan, const double* spec_d, double* p_d, void* st
                                         reinterpret_cast<cx<double>*>(p->A), a_cp, p->ycols, p->g, p->sy,
                                         tw + p->tw_off[3], tw + p->tw_off[4], nullptr, nullptr, st);
     if (e != cudaSuccess) return cuda_fail(e, "slab y inverse");
-    e = launch_xinv<double>(p->xdct, p->A, p->a_pitch, p_d, p->g, false, false, nullptr, nullptr, p->sx,
+    e = launch_xinv<double>(p->xdct, p->A, p->a_pitch, p_d, nullptr, U_P, p->g, false, false, nullptr, nullptr, p->sx,
                             tw + p->tw_off[0], tw + p->tw_off[1], tw + p->tw_off[2], nullptr, st);
     if (e != cudaSuccess) return cuda_fail(e, "slab x inverse");
     return PPF_OK;
@@ -1155,7 +1180,7 @@ int time_axis(ppf_plan* p, int axis, const FftSched& s, const double* f, double*
         if (axis == 0) {
             e = launch_xfwd<T>(p->xdct, f, nullptr, p->g, p->A, p->a_pitch, s, txh, txn, txd, nullptr, st);
             if (e == cudaSuccess)
-                e = launch_xinv<T>(p->xdct, p->A, p->a_pitch, P, p->g, false, false, nullptr, nullptr, s, txh,
+                e = launch_xinv<T>(p->xdct, p->A, p->a_pitch, P, nullptr, U_P, p->g, false, false, nullptr, nullptr, s, txh,
                                    txn, txd, nullptr, st);
         } else {
             e = launch_yfwd<T>(p->ykind, reinterpret_cast<const cx<T>*>(p->A), a_cp, reinterpret_cast<cx<T>*>(p->B),
@@ -1290,30 +1315,33 @@ int batch_init(ppf_batch* b, const ppf_desc* descs, int count, int flags, int br
     }
     // one set of work buffers per branch, sized for its largest problem
     for (int br = 0; br < nb; ++br) {
-        size_t aa = 0, ba = 0, ck = 0, pt = 0;
+        size_t aa = 0, ba = 0, ck = 0, pt = 0, ub = 0;
         for (int i : b->order[br]) {
             const ppf_plan* p = b->plans[i];
+            ub = std::max(ub, u_bytes(p));
             aa = std::max(aa, p->a_bytes);
             ba = std::max(ba, p->b_bytes);
             ck = std::max(ck, (size_t)p->ckpt_doubles);
             pt = std::max(pt, (size_t)partials_doubles(p));
         }
-        void *A = nullptr, *B = nullptr, *C = nullptr, *Pt = nullptr;
+        void *A = nullptr, *B = nullptr, *C = nullptr, *Pt = nullptr, *Uf = nullptr;
         if (cudaMalloc(&A, aa) != cudaSuccess || cudaMalloc(&B, ba) != cudaSuccess ||
             cudaMalloc(&C, sizeof(double) * std::max<size_t>(ck, 1)) != cudaSuccess ||
-            (pt && cudaMalloc(&Pt, sizeof(double) * pt) != cudaSuccess)) {
+            (pt && cudaMalloc(&Pt, sizeof(double) * pt) != cudaSuccess) ||
+            (ub && cudaMalloc(&Uf, ub) != cudaSuccess)) {
             cudaGetLastError();
-            for (void* q : { A, B, C, Pt })
+            for (void* q : { A, B, C, Pt, Uf })
                 if (q) cudaFree(q);
             return fail(PPF_ERR_NOMEM, "cannot allocate batch work memory for branch %d", br);
         }
-        for (void* q : { A, B, C, Pt })
+        for (void* q : { A, B, C, Pt, Uf })
             if (q) b->work.push_back(q);
         for (int i : b->order[br]) {
             ppf_plan* p = b->plans[i];
             p->A = A;
             p->B = B;
             p->ckpt = (double*)C;
+            p->U = u_bytes(p) ? (float*)Uf : nullptr;
             const long np = partials_doubles(p);
             p->partials = np ? (double*)Pt : nullptr;
             p->xinv_nblk = np / 3;

@@ -16,6 +16,7 @@ struct Geom {
 // Residual-input options of the x-forward pass (FP64 residual refinement).
 struct ResidIn {
     const double* P;      // current iterate, ghosted layout (interior read)
+    const float* U;       // or, when set, the FP32 first iterate (same ghosted layout)
     const double* am;     // z coefficient tables (nz)
     const double* ap;
     double ix2, iy2;      // 1/dx^2, 1/dy^2 (uniform x, y)
@@ -41,10 +42,18 @@ cudaError_t launch_yinv(int kind, const cx<T>* in, long in_pitch, cx<T>* out, lo
                         const cx<T>* tw_ny, const cx<T>* tw_dct, const double* dc_shift,
                         const int* skip_flag, cudaStream_t st);
 
-// x inverse into the ghosted output.  accumulate: P <- (P - *mean_prev) + du.
+// Where the x inverse reads and writes the iterate of a mixed solve.  The
+// first iterate is made of FP32 values, so when a refinement sweep follows it
+// is kept in an FP32 ghosted field U (half the bytes, the same values):
+// U_P      accumulate reads P, the output goes to P (every other pass)
+// U_WRITE  the output goes to U (first pass of a refining mixed solve)
+// U_ACC    accumulate reads U, the output goes to P (its first sweep)
+enum UKind { U_P = 0, U_WRITE = 1, U_ACC = 2 };
+
+// x inverse into the ghosted output.  accumulate: u <- (u - *mean_prev) + du.
 // partials (optional): per-block [sum du^2, sum u^2, sum u], 3 doubles per block.
 template <typename T>
-cudaError_t launch_xinv(bool dct, const void* in, long in_pitch, double* P, const Geom& g,
+cudaError_t launch_xinv(bool dct, const void* in, long in_pitch, double* P, float* U, int ukind, const Geom& g,
                         bool accumulate, bool stencil_ghosts, double* partials, const double* mean_prev,
                         const FftSched& sch, const cx<T>* tw_half, const cx<T>* tw_n, const cx<T>* tw_dct,
                         const int* skip_flag, cudaStream_t st, long* blocks_used = nullptr);

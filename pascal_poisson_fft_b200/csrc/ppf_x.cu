@@ -10,16 +10,34 @@
 // compile-time engine of a common length or the run-time engine.
 #include "ppf_xy_common.cuh"
 
+#include <type_traits>
+
 namespace ppf {
 
 constexpr int ct_log2(int w) { return w <= 1 ? 0 : 1 + ct_log2(w / 2); }
 constexpr int MAXW = 128;  // widest tile of any shape (FP32, n = 32)
 
+// the two values at p, p+1 (p 16-byte aligned for FP64, 8-byte for FP32)
+__device__ __forceinline__ void ld_pair_al(const double* p, double& a, double& b)
+{
+    const double2 v = __ldg(reinterpret_cast<const double2*>(p));
+    a = v.x;
+    b = v.y;
+}
+__device__ __forceinline__ void ld_pair_al(const float* p, double& a, double& b)
+{
+    const float2 v = __ldg(reinterpret_cast<const float2*>(p));
+    a = (double)v.x;
+    b = (double)v.y;
+}
+
 // --------------------------------------------------------------------------
 // x forward: real lines (FP64 input, optionally f - L u) -> half spectrum
-// (R2C, complex rows of nx/2+1) or DCT-II (real rows of nx).
+// (R2C, complex rows of nx/2+1) or DCT-II (real rows of nx).  RESID: 0 none,
+// 1 the residual of the FP64 iterate rs.P, 2 of the FP32 iterate rs.U (same
+// ghosted layout; its values are FP32 numbers, so f - L u is the same).
 // --------------------------------------------------------------------------
-template <typename T, bool DCT, bool RESID, typename SH>
+template <typename T, bool DCT, int RESID, typename SH>
 __device__ __forceinline__ void xfwd(const double* __restrict__ f, const ResidIn& rs, const Geom& g,
                                      void* __restrict__ out_, long out_pitch, const FftSched& sch, int Wrt, int lgWrt,
                                      const cx<T>* __restrict__ tw_half, const cx<T>* __restrict__ tw_n,
@@ -51,8 +69,10 @@ __device__ __forceinline__ void xfwd(const double* __restrict__ f, const ResidIn
         }
         __syncthreads();
     }
-    // f and P are 16-byte aligned (cudaMalloc'd arrays): pairs load as one vector
-    const bool vec = ((reinterpret_cast<size_t>(f) | reinterpret_cast<size_t>(rs.P)) & 15) == 0;
+    // f and the iterate are 16-byte aligned (cudaMalloc'd arrays): pairs load
+    // as one vector (the pair (2n-1, 2n) of a ghosted row starts at an even index)
+    const bool vec = ((reinterpret_cast<size_t>(f) | reinterpret_cast<size_t>(rs.P) |
+                       reinterpret_cast<size_t>(rs.U)) & 15) == 0;
     const long sy = g.pstride_y, sz = g.pstride_z;
 
     for (int e = threadIdx.x; e < E; e += NTH) {
@@ -74,12 +94,14 @@ __device__ __forceinline__ void xfwd(const double* __restrict__ f, const ResidIn
                 // f - L_h u at cells 2n and 2n+1.  The ghost cells hold the
                 // stencil's neighbours (periodic copies or wall mirrors, written
                 // by the previous x-inverse pass), so no index wraps here.
-                const double* c = rs.P + line_c[l] + 2 * n;   // c[0] = u(2n), odd offset
+                using UT = typename std::conditional<RESID == 2, float, double>::type;
+                const UT* ub;
+                if constexpr (RESID == 2) ub = rs.U; else ub = rs.P;
+                const UT* c = ub + line_c[l] + 2 * n;   // c[0] = u(2n), odd offset
                 double xm, u0, u1, xp;
                 if (vec) {
-                    const double2 lo = __ldg(reinterpret_cast<const double2*>(c - 1));
-                    const double2 hi = __ldg(reinterpret_cast<const double2*>(c + 1));
-                    xm = lo.x; u0 = lo.y; u1 = hi.x; xp = hi.y;
+                    ld_pair_al(c - 1, xm, u0);
+                    ld_pair_al(c + 1, u1, xp);
                 } else {
                     xm = c[-1]; u0 = c[0]; u1 = c[1]; xp = c[2];
                 }
@@ -184,7 +206,7 @@ __device__ __forceinline__ void xfwd(const double* __restrict__ f, const ResidIn
         const cx<T>* __restrict__ tw_dct, const int* __restrict__ skip
 #define PPF_XFWD_ARGS f, rs, g, out_, out_pitch, sch, Wrt, lgWrt, tw_half, tw_n, tw_dct, skip
 
-template <typename T, bool DCT, bool RESID, typename SH>
+template <typename T, bool DCT, int RESID, typename SH>
 __global__ void __launch_bounds__(512) k_xfwd(PPF_XFWD_PARAMS)
 {
     xfwd<T, DCT, RESID, SH>(PPF_XFWD_ARGS);
@@ -194,17 +216,29 @@ __global__ void __launch_bounds__(512) k_xfwd(PPF_XFWD_PARAMS)
 template <bool DCT, typename SH, typename T = double>
 __global__ void __launch_bounds__(SH::NT, 5) k_xfwd64(PPF_XFWD_PARAMS)
 {
-    xfwd<T, DCT, false, SH>(PPF_XFWD_ARGS);
+    xfwd<T, DCT, 0, SH>(PPF_XFWD_ARGS);
+}
+
+// The row of the ghosted iterate at offset o (elements) into L2, in bulk
+// (the copy's start and size rounded out to 16 bytes)
+template <typename U>
+__device__ __forceinline__ void prefetch_row(const U* base, long o, int n)
+{
+    const size_t a = reinterpret_cast<size_t>(base + o) & ~(size_t)15;
+    const size_t e = (reinterpret_cast<size_t>(base + o + n) + 15) & ~(size_t)15;
+    prefetch_l2(reinterpret_cast<const void*>(a), (unsigned)(e - a));
 }
 
 // --------------------------------------------------------------------------
 // x inverse: half spectrum (C2R) or DCT coefficients (inverse DCT) ->
-// interior of the ghosted FP64 output.  ACC: u <- (u - mean_prev) + du.
-// partials (optional): per-block [sum du^2, sum u^2, sum u].
+// interior of the ghosted output.  ACC: u <- (u - mean_prev) + du.
+// partials (optional): per-block [sum du^2, sum u^2, sum u].  UK (UKind):
+// U_P reads and writes the FP64 P, U_WRITE writes the FP32 field U instead
+// (values that are FP32 numbers already), U_ACC reads u from U and writes P.
 // --------------------------------------------------------------------------
-template <typename T, bool DCT, bool ACC, bool GHOST, typename SH>
+template <typename T, bool DCT, bool ACC, bool GHOST, typename SH, int UK = U_P>
 __device__ __forceinline__ void xinv(const void* __restrict__ in_, long in_pitch, double* __restrict__ P,
-                                     const Geom& g, double* __restrict__ partials,
+                                     float* __restrict__ U, const Geom& g, double* __restrict__ partials,
                                      const double* __restrict__ mean_prev, const FftSched& sch, int Wrt, int lgWrt,
                                      const cx<T>* __restrict__ tw_half, const cx<T>* __restrict__ tw_n,
                                      const cx<T>* __restrict__ tw_dct, const int* __restrict__ skip)
@@ -221,14 +255,25 @@ __device__ __forceinline__ void xinv(const void* __restrict__ in_, long in_pitch
     const long nlines = (long)g.ny * g.nz;
     const long line0 = (long)blockIdx.x * W;
     const int E = nc << lgW;
-    // the P rows this tile updates are fetched into L2 in bulk now, so that
+    // the rows of u this tile updates are fetched into L2 in bulk now, so that
     // the read-modify-write after the transform finds them there
-    if (ACC && threadIdx.x < W && (reinterpret_cast<size_t>(P) & 15) == 0) {
+    if (ACC && threadIdx.x < W) {
         const long line = line0 + threadIdx.x;
-        if (line < nlines)
-            prefetch_l2(P + (line % g.ny + 1) * g.pstride_y + (line / g.ny + 1) * g.pstride_z,
-                        (unsigned)((nx + 2) * sizeof(double)));
+        const long o = (line % g.ny + 1) * g.pstride_y + (line / g.ny + 1) * g.pstride_z;
+        if (line < nlines) {
+            if (UK == U_ACC) prefetch_row(U, o, nx + 2);
+            else prefetch_row(P, o, nx + 2);
+        }
     }
+    // the iterate read by ACC and the one written
+    auto src = [&](long o) -> double {
+        if constexpr (UK == U_ACC) return (double)U[o];
+        else return P[o];
+    };
+    auto put = [&](long o, double v) {
+        if constexpr (UK == U_WRITE) U[o] = (float)v;
+        else P[o] = v;
+    };
 
     if constexpr (!DCT) {
         // C2R split, one pair (k, nc-k) per iteration: Z_k from (X_k, conj X_{nc-k}),
@@ -328,19 +373,19 @@ __device__ __forceinline__ void xinv(const void* __restrict__ in_, long in_pitch
             // iterate (the residual cannot see constants, so the gauge is kept here)
             double u0 = x0, u1 = x1;
             if (ACC) {
-                u0 = (P[o] - mprev) + x0;
-                u1 = (P[o + 1] - mprev) + x1;
+                u0 = (src(o) - mprev) + x0;
+                u1 = (src(o + 1) - mprev) + x1;
             }
-            P[o] = u0;
-            P[o + 1] = u1;
+            put(o, u0);
+            put(o + 1, u1);
             if (GHOST) {
                 // stencil ghosts for the next residual (the reference's ghost
                 // update overwrites them after the last sweep)
-                if (n == 0) P[o + (g.px ? nx : -1)] = u0;
-                if (n == nc - 1) P[o + 1 + (g.px ? -nx : 1)] = u1;
+                if (n == 0) put(o + (g.px ? nx : -1), u0);
+                if (n == nc - 1) put(o + 1 + (g.px ? -nx : 1), u1);
                 const long gy = line_gy[l], gz = line_gz[l];
-                if (gy) { P[o + gy] = u0; P[o + 1 + gy] = u1; }
-                if (gz) { P[o + gz] = u0; P[o + 1 + gz] = u1; }
+                if (gy) { put(o + gy, u0); put(o + 1 + gy, u1); }
+                if (gz) { put(o + gz, u0); put(o + 1 + gz, u1); }
             }
             if (partials) {
                 acc_du += x0 * x0 + x1 * x1;
@@ -361,16 +406,16 @@ __device__ __forceinline__ void xinv(const void* __restrict__ in_, long in_pitch
             const long o = line_base[l] + i;
             // refinement: u <- u + du - mean(u), the FP64 mean of the previous
             // iterate (the residual cannot see constants, so the gauge is kept here)
-            const double un = ACC ? (P[o] - mprev) + x : x;
-            P[o] = un;
+            const double un = ACC ? (src(o) - mprev) + x : x;
+            put(o, un);
             if (GHOST) {
                 // stencil ghosts for the next residual (the reference's ghost
                 // update overwrites them after the last sweep)
-                if (i == 0) P[o + (g.px ? nx : -1)] = un;
-                if (i == nx - 1) P[o + (g.px ? -nx : 1)] = un;
+                if (i == 0) put(o + (g.px ? nx : -1), un);
+                if (i == nx - 1) put(o + (g.px ? -nx : 1), un);
                 const long gy = line_gy[l], gz = line_gz[l];
-                if (gy) P[o + gy] = un;
-                if (gz) P[o + gz] = un;
+                if (gy) put(o + gy, un);
+                if (gz) put(o + gz, un);
             }
             if (partials) {
                 acc_du += x * x;
@@ -402,16 +447,17 @@ __device__ __forceinline__ void xinv(const void* __restrict__ in_, long in_pitch
 }
 
 #define PPF_XINV_PARAMS                                                                                      \
-    const void* __restrict__ in_, long in_pitch, double* __restrict__ P, Geom g, double* __restrict__ partials, \
+    const void* __restrict__ in_, long in_pitch, double* __restrict__ P, float* __restrict__ U, Geom g,        \
+        double* __restrict__ partials,                                                                         \
         const double* __restrict__ mean_prev, FftSched sch, int Wrt, int lgWrt,                                \
         const cx<T>* __restrict__ tw_half, const cx<T>* __restrict__ tw_n, const cx<T>* __restrict__ tw_dct,   \
         const int* __restrict__ skip
-#define PPF_XINV_ARGS in_, in_pitch, P, g, partials, mean_prev, sch, Wrt, lgWrt, tw_half, tw_n, tw_dct, skip
+#define PPF_XINV_ARGS in_, in_pitch, P, U, g, partials, mean_prev, sch, Wrt, lgWrt, tw_half, tw_n, tw_dct, skip
 
-template <typename T, bool DCT, bool ACC, bool GHOST, typename SH>
+template <typename T, bool DCT, bool ACC, bool GHOST, typename SH, int UK = U_P>
 __global__ void __launch_bounds__(512) k_xinv(PPF_XINV_PARAMS)
 {
-    xinv<T, DCT, ACC, GHOST, SH>(PPF_XINV_ARGS);
+    xinv<T, DCT, ACC, GHOST, SH, UK>(PPF_XINV_ARGS);
 }
 
 // FP64 compile-time tiles: five resident CTAs of SH::NT threads per SM
@@ -430,9 +476,10 @@ __global__ void __launch_bounds__(SH::NT, 5) k_xinv64(PPF_XINV_PARAMS)
 // k_xinv<T, false, ACC, GHOST>.  (FP64 tiles take the non-pipelined kernel:
 // two 66 KB buffers at 128 registers leave too few resident CTAs.)
 // --------------------------------------------------------------------------
-template <typename T, bool ACC, bool GHOST, typename SH>
+template <typename T, bool ACC, bool GHOST, typename SH, int UK = U_P>
 __global__ void __launch_bounds__(SH::NT) k_xinv_pipe(const cx<T>* __restrict__ in, long in_pitch,
-                                                     double* __restrict__ P, Geom g, double* __restrict__ partials,
+                                                     double* __restrict__ P, float* __restrict__ U, Geom g,
+                                                     double* __restrict__ partials,
                                                      const double* __restrict__ mean_prev,
                                                      const cx<T>* __restrict__ tw_half,
                                                      const cx<T>* __restrict__ tw_n, const int* __restrict__ skip)
@@ -449,7 +496,14 @@ __global__ void __launch_bounds__(SH::NT) k_xinv_pipe(const cx<T>* __restrict__ 
     __shared__ long line_base[W], line_gy[W], line_gz[W];
     const long nlines = (long)g.ny * g.nz;
     const long ntiles = (nlines + W - 1) / W;
-    const bool pf = (reinterpret_cast<size_t>(P) & 15) == 0;
+    auto src = [&](long o) -> double {
+        if constexpr (UK == U_ACC) return (double)U[o];
+        else return P[o];
+    };
+    auto put = [&](long o, double v) {
+        if constexpr (UK == U_WRITE) U[o] = (float)v;
+        else P[o] = v;
+    };
     auto issue = [&](long t, cx<T>* b) {
         const long line0 = t * W;
         for (int e = threadIdx.x; e < ER; e += NT) {
@@ -469,11 +523,12 @@ __global__ void __launch_bounds__(SH::NT) k_xinv_pipe(const cx<T>* __restrict__ 
         const long tn = t + gridDim.x;
         if (tn < ntiles) issue(tn, nxt);
         else cp_async_commit();
-        // this tile's P rows into L2 ahead of the read-modify-write
-        if (ACC && pf && threadIdx.x < W && line0 + threadIdx.x < nlines) {
+        // this tile's rows of u into L2 ahead of the read-modify-write
+        if (ACC && threadIdx.x < W && line0 + threadIdx.x < nlines) {
             const long line = line0 + threadIdx.x;
-            prefetch_l2(P + (line % g.ny + 1) * g.pstride_y + (line / g.ny + 1) * g.pstride_z,
-                        (unsigned)((NX + 2) * sizeof(double)));
+            const long o = (line % g.ny + 1) * g.pstride_y + (line / g.ny + 1) * g.pstride_z;
+            if (UK == U_ACC) prefetch_row(U, o, NX + 2);
+            else prefetch_row(P, o, NX + 2);
         }
         for (int l = threadIdx.x; l < W; l += NT) {
             const long line = line0 + l;
@@ -523,17 +578,17 @@ __global__ void __launch_bounds__(SH::NT) k_xinv_pipe(const cx<T>* __restrict__ 
             const long o = line_base[l] + 2 * n;
             double u0 = x0, u1 = x1;
             if (ACC) {
-                u0 = (P[o] - mprev) + x0;
-                u1 = (P[o + 1] - mprev) + x1;
+                u0 = (src(o) - mprev) + x0;
+                u1 = (src(o + 1) - mprev) + x1;
             }
-            P[o] = u0;
-            P[o + 1] = u1;
+            put(o, u0);
+            put(o + 1, u1);
             if (GHOST) {
-                if (n == 0) P[o + (g.px ? NX : -1)] = u0;
-                if (n == NC - 1) P[o + 1 + (g.px ? -NX : 1)] = u1;
+                if (n == 0) put(o + (g.px ? NX : -1), u0);
+                if (n == NC - 1) put(o + 1 + (g.px ? -NX : 1), u1);
                 const long gy = line_gy[l], gz = line_gz[l];
-                if (gy) { P[o + gy] = u0; P[o + 1 + gy] = u1; }
-                if (gz) { P[o + gz] = u0; P[o + 1 + gz] = u1; }
+                if (gy) { put(o + gy, u0); put(o + 1 + gy, u1); }
+                if (gz) { put(o + gz, u0); put(o + 1 + gz, u1); }
             }
             if (partials) {
                 acc_du += x0 * x0 + x1 * x1;
@@ -600,24 +655,35 @@ cudaError_t launch_xfwd(bool dct, const double* f, const ResidIn* resid, const G
                 return;
             }
         }
+        if constexpr (sizeof(T) == 4) {
+            if (resid && rs.U) {
+                if (dct) go(k_xfwd<T, true, 2, SH>);
+                else go(k_xfwd<T, false, 2, SH>);
+                return;
+            }
+        }
         if (dct) {
-            if (resid) go(k_xfwd<T, true, true, SH>);
-            else go(k_xfwd<T, true, false, SH>);
+            if (resid) go(k_xfwd<T, true, 1, SH>);
+            else go(k_xfwd<T, true, 0, SH>);
         } else {
-            if (resid) go(k_xfwd<T, false, true, SH>);
-            else go(k_xfwd<T, false, false, SH>);
+            if (resid) go(k_xfwd<T, false, 1, SH>);
+            else go(k_xfwd<T, false, 0, SH>);
         }
     });
     return err;
 }
 
 template <typename T>
-cudaError_t launch_xinv(bool dct, const void* in, long in_pitch, double* P, const Geom& g, bool accumulate,
-                        bool stencil_ghosts, double* partials, const double* mean_prev, const FftSched& sch,
-                        const cx<T>* tw_half, const cx<T>* tw_n, const cx<T>* tw_dct, const int* skip_flag,
-                        cudaStream_t st, long* blocks_used)
+cudaError_t launch_xinv(bool dct, const void* in, long in_pitch, double* P, float* U, int ukind, const Geom& g,
+                        bool accumulate, bool stencil_ghosts, double* partials, const double* mean_prev,
+                        const FftSched& sch, const cx<T>* tw_half, const cx<T>* tw_n, const cx<T>* tw_dct,
+                        const int* skip_flag, cudaStream_t st, long* blocks_used)
 {
     const int nc = g.nx / 2;
+    // the FP32 iterate belongs to the refinement of FP32 spectra: U_WRITE
+    // with stencil ghosts and no accumulate, U_ACC with both
+    if (ukind != U_P && (sizeof(T) != 4 || !U || !stencil_ghosts || accumulate != (ukind == U_ACC)))
+        return cudaErrorInvalidValue;
     cudaError_t err = cudaSuccess;
     with_shape<T>(sch, [&](auto sh) {
         using SH = decltype(sh);
@@ -630,7 +696,7 @@ cudaError_t launch_xinv(bool dct, const void* in, long in_pitch, double* P, cons
         auto go = [&](auto kern) {
             err = set_smem(kern, smem);
             if (err != cudaSuccess) return;
-            kern<<<grid, threads, smem, st>>>(in, in_pitch, P, g, partials, mean_prev, sch, W, ilog2i(W), tw_half,
+            kern<<<grid, threads, smem, st>>>(in, in_pitch, P, U, g, partials, mean_prev, sch, W, ilog2i(W), tw_half,
                                               tw_n, tw_dct, skip_flag);
             err = cudaGetLastError();
         };
@@ -643,11 +709,13 @@ cudaError_t launch_xinv(bool dct, const void* in, long in_pitch, double* P, cons
                     if (err == cudaSuccess) err = persistent_grid(kern, SH::NT, psmem, (long)grid.x, &pgrid);
                     if (err != cudaSuccess) return;
                     if (blocks_used) *blocks_used = pgrid;
-                    kern<<<pgrid, SH::NT, psmem, st>>>(reinterpret_cast<const cx<T>*>(in), in_pitch, P, g, partials,
-                                                      mean_prev, tw_half, tw_n, skip_flag);
+                    kern<<<pgrid, SH::NT, psmem, st>>>(reinterpret_cast<const cx<T>*>(in), in_pitch, P, U, g,
+                                                      partials, mean_prev, tw_half, tw_n, skip_flag);
                     err = cudaGetLastError();
                 };
-                if (!stencil_ghosts) pipe(k_xinv_pipe<T, false, false, SH>);
+                if (ukind == U_WRITE) pipe(k_xinv_pipe<T, false, true, SH, U_WRITE>);
+                else if (ukind == U_ACC) pipe(k_xinv_pipe<T, true, true, SH, U_ACC>);
+                else if (!stencil_ghosts) pipe(k_xinv_pipe<T, false, false, SH>);
                 else if (accumulate) pipe(k_xinv_pipe<T, true, true, SH>);
                 else pipe(k_xinv_pipe<T, false, true, SH>);
                 return;
@@ -657,6 +725,18 @@ cudaError_t launch_xinv(bool dct, const void* in, long in_pitch, double* P, cons
             if (!stencil_ghosts && !accumulate) {
                 if (dct) go(k_xinv64<true, SH>);
                 else go(k_xinv64<false, SH>);
+                return;
+            }
+        }
+        if constexpr (sizeof(T) == 4) {
+            if (ukind == U_WRITE) {
+                if (dct) go(k_xinv<T, true, false, true, SH, U_WRITE>);
+                else go(k_xinv<T, false, false, true, SH, U_WRITE>);
+                return;
+            }
+            if (ukind == U_ACC) {
+                if (dct) go(k_xinv<T, true, true, true, SH, U_ACC>);
+                else go(k_xinv<T, false, true, true, SH, U_ACC>);
                 return;
             }
         }
@@ -697,7 +777,8 @@ template long xinv_blocks<float>(const Geom&, const FftSched&);
     template cudaError_t launch_xfwd<T>(bool, const double*, const ResidIn*, const Geom&, void*, long,     \
                                         const FftSched&, const cx<T>*, const cx<T>*, const cx<T>*,         \
                                         const int*, cudaStream_t);                                         \
-    template cudaError_t launch_xinv<T>(bool, const void*, long, double*, const Geom&, bool, bool,        \
+    template cudaError_t launch_xinv<T>(bool, const void*, long, double*, float*, int, const Geom&, bool,  \
+                                        bool,                                                              \
                                         double*, const double*, const FftSched&, const cx<T>*,             \
                                         const cx<T>*, const cx<T>*, const int*, cudaStream_t, long*);
 PPF_INST(double)

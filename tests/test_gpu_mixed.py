@@ -93,3 +93,32 @@ def test_mixed_lowk_systems(shape, pbc, lowk):
     P = gpu_solve(p, precision=PPF_MIXED, max_sweeps=3, lowk_threshold=lowk)
     assert rel_l2(P, ref) < TOL_MIXED
     assert rel_l2(gpu_solve(p, precision=PPF_FP32, lowk_threshold=lowk), ref) < TOL_FP32
+
+
+# A refining mixed solve keeps its first iterate (FP32 values) in an FP32
+# ghosted field instead of P: the first sweep's residual and accumulate read
+# it from there.  Every boundary pair, compile-time and run-time x lengths,
+# no sweep (the iterate goes straight to P), one and two sweeps.
+@pytest.mark.parametrize("shape,pbc", [
+    ((64, 48, 40), (1, 1, 0)),
+    ((64, 48, 40), (0, 0, 0)),
+    ((40, 36, 24), (1, 0, 0)),
+    ((48, 40, 37), (0, 1, 0)),
+])
+def test_mixed_fp32_first_iterate(shape, pbc):
+    import pascal_poisson_fft_b200 as ppf
+    rng = np.random.default_rng(5)
+    p = W.random_problem(rng, *shape, pbc, beta=1.5)
+    ref = oracle_solve(p)
+    e0 = rel_l2(gpu_solve(p, precision=PPF_MIXED, max_sweeps=0), ref)
+    e1 = rel_l2(gpu_solve(p, precision=PPF_MIXED, max_sweeps=1), ref)
+    e2 = rel_l2(gpu_solve(p, precision=PPF_MIXED, max_sweeps=2), ref)
+    assert e0 < TOL_FP32
+    assert e1 < 1e-8 and e1 < e0 * 1e-3
+    assert e2 < TOL_MIXED
+    n1, n2, n3 = shape
+    mk = lambda s: ppf.Plan(n1, n2, n3, p.L1, p.L2, *pbc, precision=PPF_MIXED, max_sweeps=s)
+    a, b = mk(0), mk(1)
+    assert b.workspace_bytes() - a.workspace_bytes() == 4 * (n1 + 2) * (n2 + 2) * (n3 + 2)
+    a.close()
+    b.close()
