@@ -153,6 +153,39 @@ template <typename T, bool INV> struct Dft<T, INV, 16> {
     }
 };
 
+// The twiddles w^r (r = 1..R-1, w = tw[k ts]) of one butterfly applied to
+// its inputs v[1..R-1].  FP64 reads every power from the table.  FP32 reads
+// w and forms w^2 = w w, w^3 = w w^2, w^4 = w^2 w^2, w^5 = w^4 w,
+// w^6 = w^4 w^2, w^7 = w^4 w^3 (at most three products deep, a few ulp of
+// FP32, which the FP64 refinement absorbs): one load instead of R-1 in the
+// passes the FP32 y kernels are bound by.
+template <typename T, bool INV, int R>
+__device__ __forceinline__ void twiddle_mul(cx<T>* v, const cx<T>* __restrict__ tw, int k, int ts)
+{
+    if constexpr (sizeof(T) == 4 && (R == 4 || R == 5 || R == 8)) {
+        cx<T> w[R];
+        w[1] = ldg(tw + k * ts);
+        if (INV) w[1].y = -w[1].y;
+        w[2] = cmul(w[1], w[1]);
+        w[3] = cmul(w[1], w[2]);
+        if constexpr (R >= 5) w[4] = cmul(w[2], w[2]);
+        if constexpr (R == 8) {
+            w[5] = cmul(w[4], w[1]);
+            w[6] = cmul(w[4], w[2]);
+            w[7] = cmul(w[4], w[3]);
+        }
+#pragma unroll
+        for (int r = 1; r < R; ++r) v[r] = cmul(v[r], w[r]);
+    } else {
+#pragma unroll
+        for (int r = 1; r < R; ++r) {
+            cx<T> w = ldg(tw + r * k * ts);
+            if (INV) w.y = -w.y;
+            v[r] = cmul(v[r], w);
+        }
+    }
+}
+
 // One Stockham pass of radix R over the W-line tile.  tw[k] = e^{-2 pi i k/n}.
 // v is the caller's register buffer (VMAX complex), shared by every radix so
 // that all passes reuse the same registers.
@@ -183,14 +216,7 @@ __device__ __forceinline__ void fft_pass(cx<T>* s, int n, int W, int lgW, int Ns
         if (t < items) {
             const int l = t & (W - 1), j = t >> lgW;
             const int k = j % Ns;
-            if (Ns > 1) {
-#pragma unroll
-                for (int r = 1; r < R; ++r) {
-                    cx<T> w = ldg(tw + r * k * tstride);
-                    if (INV) w.y = -w.y;
-                    v[q * R + r] = cmul(v[q * R + r], w);
-                }
-            }
+            if (Ns > 1) twiddle_mul<T, INV, R>(v + q * R, tw, k, tstride);
             Dft<T, INV, R>::run(v + q * R);
             const int base = (j - k) * R + k;
 #pragma unroll
@@ -258,14 +284,7 @@ __device__ __forceinline__ void fft_pass_ct(cx<T>* s, const cx<T>* __restrict__ 
         if (ITEMS % NT == 0 || t < ITEMS) {
             const int l = t % W, j = t / W;
             const int k = j % NS;
-            if (NS > 1) {
-#pragma unroll
-                for (int r = 1; r < R; ++r) {
-                    cx<T> w = ldg(tw + r * k * TS);
-                    if (INV) w.y = -w.y;
-                    v[q * R + r] = cmul(v[q * R + r], w);
-                }
-            }
+            if (NS > 1) twiddle_mul<T, INV, R>(v + q * R, tw, k, TS);
             Dft<T, INV, R>::run(v + q * R);
             const int base = (j - k) * R + k;
 #pragma unroll
