@@ -17,6 +17,16 @@ namespace ppf {
 constexpr int ct_log2(int w) { return w <= 1 ? 0 : 1 + ct_log2(w / 2); }
 constexpr int MAXW = 128;  // widest tile of any shape (FP32, n = 32)
 
+// n elements at base + o into L2, in bulk: the 16-byte aligned part of the
+// range (start rounded up, end rounded down), so the copy never leaves it
+template <typename U>
+__device__ __forceinline__ void prefetch_row(const U* base, long o, int n)
+{
+    const size_t a = (reinterpret_cast<size_t>(base + o) + 15) & ~(size_t)15;
+    const size_t e = reinterpret_cast<size_t>(base + o + n) & ~(size_t)15;
+    if (e > a) prefetch_l2(reinterpret_cast<const void*>(a), (unsigned)(e - a));
+}
+
 // the two values at p, p+1 (p 16-byte aligned for FP64, 8-byte for FP32)
 __device__ __forceinline__ void ld_pair_al(const double* p, double& a, double& b)
 {
@@ -68,6 +78,18 @@ __device__ __forceinline__ void xfwd(const double* __restrict__ f, const ResidIn
             line_ap[l] = (k < g.nz) ? rs.ap[k] : 0.0;
         }
         __syncthreads();
+    }
+    // this tile's rows of f (and the iterate's rows of its lines) into L2 in
+    // bulk, so the loads below wait on L2, not on HBM: one warp issues few
+    // loads at a time and the tile's 64 KB would otherwise trickle in
+    if (threadIdx.x < W && line0 + threadIdx.x < nlines) {
+        const long line = line0 + threadIdx.x;
+        prefetch_row(f, line * nx, nx);
+        if constexpr (RESID != 0) {
+            const long o = (line % g.ny + 1) * g.pstride_y + (line / g.ny + 1) * g.pstride_z;
+            if constexpr (RESID == 2) prefetch_row(rs.U, o, nx + 2);
+            else prefetch_row(rs.P, o, nx + 2);
+        }
     }
     // f and the iterate are 16-byte aligned (cudaMalloc'd arrays): pairs load
     // as one vector (the pair (2n-1, 2n) of a ghosted row starts at an even index)
@@ -217,16 +239,6 @@ template <bool DCT, typename SH, typename T = double>
 __global__ void __launch_bounds__(SH::NT, 5) k_xfwd64(PPF_XFWD_PARAMS)
 {
     xfwd<T, DCT, 0, SH>(PPF_XFWD_ARGS);
-}
-
-// The row of the ghosted iterate at offset o (elements) into L2, in bulk
-// (the copy's start and size rounded out to 16 bytes)
-template <typename U>
-__device__ __forceinline__ void prefetch_row(const U* base, long o, int n)
-{
-    const size_t a = reinterpret_cast<size_t>(base + o) & ~(size_t)15;
-    const size_t e = (reinterpret_cast<size_t>(base + o + n) + 15) & ~(size_t)15;
-    prefetch_l2(reinterpret_cast<const void*>(a), (unsigned)(e - a));
 }
 
 // --------------------------------------------------------------------------
