@@ -267,6 +267,12 @@ __device__ __forceinline__ void xinv(const void* __restrict__ in_, long in_pitch
     const long nlines = (long)g.ny * g.nz;
     const long line0 = (long)blockIdx.x * W;
     const int E = nc << lgW;
+    // the tile's spectral rows into L2 in bulk
+    if (threadIdx.x < W && line0 + threadIdx.x < nlines) {
+        const long line = line0 + threadIdx.x;
+        if (DCT) prefetch_row(reinterpret_cast<const T*>(in_), line * in_pitch, nx);
+        else prefetch_row(reinterpret_cast<const cx<T>*>(in_), line * in_pitch, nc + 1);
+    }
     // the rows of u this tile updates are fetched into L2 in bulk now, so that
     // the read-modify-write after the transform finds them there
     if (ACC && threadIdx.x < W) {

@@ -68,7 +68,7 @@ void with_shape(const FftSched& sch, F&& f)
             case 32:  f(ShapeCT<32, 128, 256, 8, 4>{}); return;
             case 64:  f(ShapeCT<64, 64, 256, 8, 8>{}); return;
             case 128: f(ShapeCT<128, 32, 256, 8, 4, 4>{}); return;
-            case 256: f(ShapeCT<256, 16, 256, 8, 8, 4>{}); return;
+            case 256: f(ShapeCT<256, 8, 256, 8, 8, 4>{}); return;
             case 384: f(ShapeCT<384, 16, 384, 8, 4, 4, 3>{}); return;
             case 512: f(ShapeCT<512, 16, 512, 8, 8, 8>{}); return;
             case 768: f(ShapeCT<768, 8, 384, 8, 8, 4, 3>{}); return;

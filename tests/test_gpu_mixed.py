@@ -104,6 +104,8 @@ def test_mixed_lowk_systems(shape, pbc, lowk):
     ((64, 48, 40), (0, 0, 0)),
     ((40, 36, 24), (1, 0, 0)),
     ((48, 40, 37), (0, 1, 0)),
+    ((512, 512, 24), (1, 1, 0)),
+    ((512, 256, 16), (0, 1, 0)),
 ])
 def test_mixed_fp32_first_iterate(shape, pbc):
     import pascal_poisson_fft_b200 as ppf
