@@ -241,6 +241,25 @@ __global__ void __launch_bounds__(SH::NT, 5) k_xfwd64(PPF_XFWD_PARAMS)
     xfwd<T, DCT, 0, SH>(PPF_XFWD_ARGS);
 }
 
+// The x stencil ghosts of a tile's lines (the periodic copy, or the wall
+// mirror, of each line's first and last interior value), copied after the
+// tile's interior values are written and visible to the block: the value a
+// ghost receives is the one just stored, in every iterate kind.
+template <int UK>
+__device__ __forceinline__ void x_ghosts(double* __restrict__ P, float* __restrict__ U, const Geom& g, long line0,
+                                         int W, long nlines, int nx)
+{
+    for (int t = threadIdx.x; t < 2 * W; t += blockDim.x) {
+        const long line = line0 + (t >> 1);
+        if (line >= nlines) continue;
+        const long ob = 1 + (line % g.ny + 1) * g.pstride_y + (line / g.ny + 1) * g.pstride_z;
+        const long from = (t & 1) ? ob + nx - 1 : ob;
+        const long to = (t & 1) ? from + (g.px ? -nx : 1) : from + (g.px ? nx : -1);
+        if constexpr (UK == U_WRITE) U[to] = U[from];
+        else P[to] = P[from];
+    }
+}
+
 // --------------------------------------------------------------------------
 // x inverse: half spectrum (C2R) or DCT coefficients (inverse DCT) ->
 // interior of the ghosted output.  ACC: u <- (u - mean_prev) + du.
@@ -356,6 +375,7 @@ __device__ __forceinline__ void xinv(const void* __restrict__ in_, long in_pitch
     // ghosted-output offset of each line of the tile, and (GHOST) the offsets
     // of the ghost lines its values are copied to (0: none)
     __shared__ long line_base[MAXW], line_gy[MAXW], line_gz[MAXW];
+    bool has_yz = false;
     for (int l = threadIdx.x; l < W; l += NTH) {
         const long line = line0 + l;
         const long j = line % g.ny, k = line / g.ny;
@@ -371,9 +391,11 @@ __device__ __forceinline__ void xinv(const void* __restrict__ in_, long in_pitch
             else if (k == g.nz - 1) gz = g.pstride_z;
             line_gy[l] = gy;
             line_gz[l] = gz;
+            has_yz |= (line < nlines) && (gy || gz);
         }
     }
-    __syncthreads();
+    // whether any line of the tile has y or z ghosts (most tiles have none)
+    const bool yz = __syncthreads_or(has_yz);
     tile_fft<T, true, SH>(s, sch, W, lgW, tw_half);
 
     double acc_du = 0.0, acc_u = 0.0, acc_s = 0.0;
@@ -396,11 +418,9 @@ __device__ __forceinline__ void xinv(const void* __restrict__ in_, long in_pitch
             }
             put(o, u0);
             put(o + 1, u1);
-            if (GHOST) {
-                // stencil ghosts for the next residual (the reference's ghost
-                // update overwrites them after the last sweep)
-                if (n == 0) put(o + (g.px ? nx : -1), u0);
-                if (n == nc - 1) put(o + 1 + (g.px ? -nx : 1), u1);
+            if (GHOST && yz) {
+                // y and z stencil ghosts for the next residual (the reference's
+                // ghost update overwrites them after the last sweep)
                 const long gy = line_gy[l], gz = line_gz[l];
                 if (gy) { put(o + gy, u0); put(o + 1 + gy, u1); }
                 if (gz) { put(o + gz, u0); put(o + 1 + gz, u1); }
@@ -426,11 +446,9 @@ __device__ __forceinline__ void xinv(const void* __restrict__ in_, long in_pitch
             // iterate (the residual cannot see constants, so the gauge is kept here)
             const double un = ACC ? (src(o) - mprev) + x : x;
             put(o, un);
-            if (GHOST) {
-                // stencil ghosts for the next residual (the reference's ghost
-                // update overwrites them after the last sweep)
-                if (i == 0) put(o + (g.px ? nx : -1), un);
-                if (i == nx - 1) put(o + (g.px ? -nx : 1), un);
+            if (GHOST && yz) {
+                // y and z stencil ghosts for the next residual (the reference's
+                // ghost update overwrites them after the last sweep)
                 const long gy = line_gy[l], gz = line_gz[l];
                 if (gy) put(o + gy, un);
                 if (gz) put(o + gz, un);
@@ -441,6 +459,10 @@ __device__ __forceinline__ void xinv(const void* __restrict__ in_, long in_pitch
                 acc_s += un;
             }
         }
+    }
+    if (GHOST) {
+        __syncthreads();
+        x_ghosts<UK>(P, U, g, line0, W, nlines, nx);
     }
     if (partials) {
         // deterministic per-block partial sums (reduced in a fixed order by the gate)
@@ -548,6 +570,7 @@ __global__ void __launch_bounds__(SH::NT) k_xinv_pipe(const cx<T>* __restrict__ 
             if (UK == U_ACC) prefetch_row(U, o, NX + 2);
             else prefetch_row(P, o, NX + 2);
         }
+        bool has_yz = false;
         for (int l = threadIdx.x; l < W; l += NT) {
             const long line = line0 + l;
             const long j = line % g.ny, k = line / g.ny;
@@ -561,10 +584,12 @@ __global__ void __launch_bounds__(SH::NT) k_xinv_pipe(const cx<T>* __restrict__ 
                 else if (k == g.nz - 1) gz = g.pstride_z;
                 line_gy[l] = gy;
                 line_gz[l] = gz;
+                has_yz |= (line < nlines) && (gy || gz);
             }
         }
         cp_async_wait<1>();  // this thread's copies of tile t have landed
-        __syncthreads();
+        // whether any line of the tile has y or z ghosts (most tiles have none)
+        const bool yz = __syncthreads_or(has_yz);
         // C2R split in place, one pair (k, nc-k) per iteration
         for (int e = threadIdx.x; e < (NC / 2 + 1) * W; e += NT) {
             const int l = e & (W - 1), k = e >> LGW;
@@ -601,9 +626,7 @@ __global__ void __launch_bounds__(SH::NT) k_xinv_pipe(const cx<T>* __restrict__ 
             }
             put(o, u0);
             put(o + 1, u1);
-            if (GHOST) {
-                if (n == 0) put(o + (g.px ? NX : -1), u0);
-                if (n == NC - 1) put(o + 1 + (g.px ? -NX : 1), u1);
+            if (GHOST && yz) {
                 const long gy = line_gy[l], gz = line_gz[l];
                 if (gy) { put(o + gy, u0); put(o + 1 + gy, u1); }
                 if (gz) { put(o + gz, u0); put(o + 1 + gz, u1); }
@@ -615,6 +638,7 @@ __global__ void __launch_bounds__(SH::NT) k_xinv_pipe(const cx<T>* __restrict__ 
             }
         }
         __syncthreads();  // cur and the line tables are refilled
+        if (GHOST) x_ghosts<UK>(P, U, g, line0, W, nlines, NX);
         cx<T>* tmp = cur;
         cur = nxt;
         nxt = tmp;
