@@ -11,6 +11,8 @@
 #pragma once
 #include "ppf_common.cuh"
 
+#include <type_traits>
+
 namespace ppf {
 
 template <typename T> struct K;
@@ -260,8 +262,13 @@ __device__ __forceinline__ int sidx_ct(int n, int l)
     return n * W + (l ^ (n & MASK));
 }
 
-template <typename T, bool INV, int N, int W, int NT, int R, int NS>
-__device__ __forceinline__ void fft_pass_ct(cx<T>* s, const cx<T>* __restrict__ tw)
+// Marker loader of fft_pass_ct: the pass reads its inputs from the tile.
+struct TileLd {};
+
+// LD: the inputs of the pass come from ld(n, l) instead of the tile (the
+// first pass of a transform whose input is formed on the fly)
+template <typename T, bool INV, int N, int W, int NT, int R, int NS, typename LD = TileLd>
+__device__ __forceinline__ void fft_pass_ct(cx<T>* s, const cx<T>* __restrict__ tw, LD ld = LD{})
 {
     constexpr int NB = N / R;
     constexpr int ITEMS = NB * W;
@@ -274,7 +281,10 @@ __device__ __forceinline__ void fft_pass_ct(cx<T>* s, const cx<T>* __restrict__ 
         if (ITEMS % NT == 0 || t < ITEMS) {
             const int l = t % W, j = t / W;
 #pragma unroll
-            for (int r = 0; r < R; ++r) v[q * R + r] = s[sidx_ct<T, W>(j + r * NB, l)];
+            for (int r = 0; r < R; ++r) {
+                if constexpr (std::is_same<LD, TileLd>::value) v[q * R + r] = s[sidx_ct<T, W>(j + r * NB, l)];
+                else v[q * R + r] = ld(j + r * NB, l);
+            }
         }
     }
     __syncthreads();
@@ -304,6 +314,14 @@ __device__ __forceinline__ void fft_ct_passes(cx<T>* s, const cx<T>* __restrict_
     fft_ct_passes<T, INV, N, W, NT, NS * R0, RS...>(s, tw);
 }
 
+// First pass with a loader, then the remaining passes of the radix sequence
+template <typename T, bool INV, int N, int W, int NT, typename LD, int R0, int... RS>
+__device__ __forceinline__ void fft_ct_first_ld(cx<T>* s, const cx<T>* __restrict__ tw, LD ld)
+{
+    fft_pass_ct<T, INV, N, W, NT, R0, 1, LD>(s, tw, ld);
+    fft_ct_passes<T, INV, N, W, NT, R0, RS...>(s, tw);
+}
+
 // Tile shapes.  ShapeRT: everything at run time (fft_tile).  ShapeCT: a
 // fixed length N = product of RS, W lines, NT threads per CTA.
 struct ShapeRT {
@@ -318,6 +336,14 @@ struct ShapeCT {
     static __device__ __forceinline__ void fft(cx<T>* s, const cx<T>* __restrict__ tw)
     {
         fft_ct_passes<T, INV, N_, W_, NT_, 1, RS...>(s, tw);
+    }
+    // the same transform with the first pass reading ld(n, l); the caller
+    // synchronises before (ld's sources ready), the first pass's barrier
+    // separates every ld from the in-place stores
+    template <typename T, bool INV, typename LD>
+    static __device__ __forceinline__ void fft_ld(cx<T>* s, const cx<T>* __restrict__ tw, LD ld)
+    {
+        fft_ct_first_ld<T, INV, N_, W_, NT_, LD, RS...>(s, tw, ld);
     }
 };
 

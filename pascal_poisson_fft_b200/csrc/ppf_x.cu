@@ -590,29 +590,19 @@ __global__ void __launch_bounds__(SH::NT) k_xinv_pipe(const cx<T>* __restrict__ 
         cp_async_wait<1>();  // this thread's copies of tile t have landed
         // whether any line of the tile has y or z ghosts (most tiles have none)
         const bool yz = __syncthreads_or(has_yz);
-        // C2R split in place, one pair (k, nc-k) per iteration
-        for (int e = threadIdx.x; e < (NC / 2 + 1) * W; e += NT) {
-            const int l = e & (W - 1), k = e >> LGW;
-            const int kc = NC - k;
-            cx<T> xk = cur[sidx_ct<T, W>(k, l)];
-            cx<T> xc = cur[sidx_ct<T, W>(kc, l)];
-            if (k == 0) { xk.y = (T)0; xc.y = (T)0; }
-            const cx<T> wk = ldg(tw_n + k), wc = ldg(tw_n + kc);
-            {
-                const cx<T> a = xk, b = conj(xc);
-                const cx<T> Ev = a + b, D = a - b;
-                const cx<T> O = cmul(D, conj(wk));
-                cur[sidx_ct<T, W>(k, l)] = mk<T>(Ev.x - O.y, Ev.y + O.x);
-            }
-            if (k != 0 && kc != k) {
-                const cx<T> a = xc, b = conj(xk);
-                const cx<T> Ev = a + b, D = a - b;
-                const cx<T> O = cmul(D, conj(wc));
-                cur[sidx_ct<T, W>(kc, l)] = mk<T>(Ev.x - O.y, Ev.y + O.x);
-            }
-        }
-        __syncthreads();
-        SH::template fft<T, true>(cur, tw_half);
+        // the C2R split, Z_m from (X_m, conj X_{nc-m}) with w_m, formed as the
+        // first FFT pass loads its inputs (X_0 and X_nc enter with zero
+        // imaginary parts)
+        auto zsplit = [&](int m, int l) -> cx<T> {
+            cx<T> a = cur[sidx_ct<T, W>(m, l)];
+            cx<T> xc = cur[sidx_ct<T, W>(NC - m, l)];
+            if (m == 0) { a.y = (T)0; xc.y = (T)0; }
+            const cx<T> b = conj(xc);
+            const cx<T> Ev = a + b, D = a - b;
+            const cx<T> O = cmul(D, conj(ldg(tw_n + m)));
+            return mk<T>(Ev.x - O.y, Ev.y + O.x);
+        };
+        SH::template fft_ld<T, true>(cur, tw_half, zsplit);
         for (int e = threadIdx.x; e < NC * W; e += NT) {
             const int l = e / NC, n = e - l * NC;
             if (line0 + l >= nlines) continue;
