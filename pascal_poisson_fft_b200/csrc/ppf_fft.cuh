@@ -262,13 +262,17 @@ __device__ __forceinline__ int sidx_ct(int n, int l)
     return n * W + (l ^ (n & MASK));
 }
 
-// Marker loader of fft_pass_ct: the pass reads its inputs from the tile.
+// Marker loader and storer of fft_pass_ct: the pass reads its inputs from
+// and writes its outputs to the tile.
 struct TileLd {};
+struct TileSt {};
 
 // LD: the inputs of the pass come from ld(n, l) instead of the tile (the
-// first pass of a transform whose input is formed on the fly)
-template <typename T, bool INV, int N, int W, int NT, int R, int NS, typename LD = TileLd>
-__device__ __forceinline__ void fft_pass_ct(cx<T>* s, const cx<T>* __restrict__ tw, LD ld = LD{})
+// first pass of a transform whose input is formed on the fly).  ST: the
+// outputs go to st(n, l, value) instead of the tile (the last pass of a
+// transform whose output is stored straight to global memory).
+template <typename T, bool INV, int N, int W, int NT, int R, int NS, typename LD = TileLd, typename ST = TileSt>
+__device__ __forceinline__ void fft_pass_ct(cx<T>* s, const cx<T>* __restrict__ tw, LD ld = LD{}, ST st = ST{})
 {
     constexpr int NB = N / R;
     constexpr int ITEMS = NB * W;
@@ -298,7 +302,10 @@ __device__ __forceinline__ void fft_pass_ct(cx<T>* s, const cx<T>* __restrict__ 
             Dft<T, INV, R>::run(v + q * R);
             const int base = (j - k) * R + k;
 #pragma unroll
-            for (int r = 0; r < R; ++r) s[sidx_ct<T, W>(base + r * NS, l)] = v[q * R + r];
+            for (int r = 0; r < R; ++r) {
+                if constexpr (std::is_same<ST, TileSt>::value) s[sidx_ct<T, W>(base + r * NS, l)] = v[q * R + r];
+                else st(base + r * NS, l, v[q * R + r]);
+            }
         }
     }
     __syncthreads();
@@ -322,6 +329,18 @@ __device__ __forceinline__ void fft_ct_first_ld(cx<T>* s, const cx<T>* __restric
     fft_ct_passes<T, INV, N, W, NT, R0, RS...>(s, tw);
 }
 
+// Every pass of a radix sequence, the last one handing its outputs to st
+template <typename T, bool INV, int N, int W, int NT, int NS, typename ST, int R0, int... RS>
+__device__ __forceinline__ void fft_ct_last_st(cx<T>* s, const cx<T>* __restrict__ tw, ST st)
+{
+    if constexpr (sizeof...(RS) == 0) {
+        fft_pass_ct<T, INV, N, W, NT, R0, NS, TileLd, ST>(s, tw, TileLd{}, st);
+    } else {
+        fft_pass_ct<T, INV, N, W, NT, R0, NS>(s, tw);
+        fft_ct_last_st<T, INV, N, W, NT, NS * R0, ST, RS...>(s, tw, st);
+    }
+}
+
 // Tile shapes.  ShapeRT: everything at run time (fft_tile).  ShapeCT: a
 // fixed length N = product of RS, W lines, NT threads per CTA.
 struct ShapeRT {
@@ -336,6 +355,14 @@ struct ShapeCT {
     static __device__ __forceinline__ void fft(cx<T>* s, const cx<T>* __restrict__ tw)
     {
         fft_ct_passes<T, INV, N_, W_, NT_, 1, RS...>(s, tw);
+    }
+    // the same transform with the last pass handing output n of line l to
+    // st(n, l, value) instead of the tile; every read of the tile is done
+    // when it returns (the last pass ends with a barrier)
+    template <typename T, bool INV, typename ST>
+    static __device__ __forceinline__ void fft_st(cx<T>* s, const cx<T>* __restrict__ tw, ST st)
+    {
+        fft_ct_last_st<T, INV, N_, W_, NT_, 1, ST, RS...>(s, tw, st);
     }
     // the same transform with the first pass reading ld(n, l); the caller
     // synchronises before (ld's sources ready), the first pass's barrier

@@ -218,15 +218,14 @@ __device__ __forceinline__ void y_c2c_pipe(const cx<T>* __restrict__ in, long in
         // (element (0,0) is copied by thread 0)
         if (INV && dc_shift && col0 == 0 && threadIdx.x == 0) cur[sidx_ct<T, W>(0, 0)].x -= (T)*dc_shift;
         __syncthreads();
-        SH::template fft<T, INV>(cur, tw);
+        // the last pass stores the tile's rows straight to the output (a warp
+        // writes whole W-column row segments, as a copy-out loop would); the
+        // tile is free for the refill two tiles on when the transform returns
         cx<T>* outp = out + (long)z * N * out_pitch + col0;
-#pragma unroll
-        for (int i = 0; i < EPT; ++i) {
-            const int e = threadIdx.x + i * NT;
-            const int l = e & (W - 1), k = e >> LGW;
-            if (col0 + l < ncols) outp[(long)k * out_pitch + l] = cur[sidx_ct<T, W>(k, l)];
-        }
-        __syncthreads();  // cur is refilled two tiles on
+        auto yst = [&](int k, int l, cx<T> v) {
+            if (col0 + l < ncols) outp[(long)k * out_pitch + l] = v;
+        };
+        SH::template fft_st<T, INV>(cur, tw, yst);
         cx<T>* tmp = cur;
         cur = nxt;
         nxt = tmp;
