@@ -270,8 +270,12 @@ struct TileSt {};
 // LD: the inputs of the pass come from ld(n, l) instead of the tile (the
 // first pass of a transform whose input is formed on the fly).  ST: the
 // outputs go to st(n, l, value) instead of the tile (the last pass of a
-// transform whose output is stored straight to global memory).
-template <typename T, bool INV, int N, int W, int NT, int R, int NS, typename LD = TileLd, typename ST = TileSt>
+// transform whose output is stored straight to global memory).  JF: the
+// butterflies are assigned position-fastest (consecutive threads take
+// consecutive j of one line) instead of line-fastest; in a last pass that
+// makes a warp's outputs consecutive points of one line.
+template <typename T, bool INV, int N, int W, int NT, int R, int NS, typename LD = TileLd, typename ST = TileSt,
+          bool JF = false>
 __device__ __forceinline__ void fft_pass_ct(cx<T>* s, const cx<T>* __restrict__ tw, LD ld = LD{}, ST st = ST{})
 {
     constexpr int NB = N / R;
@@ -283,7 +287,7 @@ __device__ __forceinline__ void fft_pass_ct(cx<T>* s, const cx<T>* __restrict__ 
     for (int q = 0; q < Q; ++q) {
         const int t = threadIdx.x + q * NT;
         if (ITEMS % NT == 0 || t < ITEMS) {
-            const int l = t % W, j = t / W;
+            const int l = JF ? t / NB : t % W, j = JF ? t % NB : t / W;
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 if constexpr (std::is_same<LD, TileLd>::value) v[q * R + r] = s[sidx_ct<T, W>(j + r * NB, l)];
@@ -296,7 +300,7 @@ __device__ __forceinline__ void fft_pass_ct(cx<T>* s, const cx<T>* __restrict__ 
     for (int q = 0; q < Q; ++q) {
         const int t = threadIdx.x + q * NT;
         if (ITEMS % NT == 0 || t < ITEMS) {
-            const int l = t % W, j = t / W;
+            const int l = JF ? t / NB : t % W, j = JF ? t % NB : t / W;
             const int k = j % NS;
             if (NS > 1) twiddle_mul<T, INV, R>(v + q * R, tw, k, TS);
             Dft<T, INV, R>::run(v + q * R);
@@ -321,12 +325,19 @@ __device__ __forceinline__ void fft_ct_passes(cx<T>* s, const cx<T>* __restrict_
     fft_ct_passes<T, INV, N, W, NT, NS * R0, RS...>(s, tw);
 }
 
-// First pass with a loader, then the remaining passes of the radix sequence
-template <typename T, bool INV, int N, int W, int NT, typename LD, int R0, int... RS>
-__device__ __forceinline__ void fft_ct_first_ld(cx<T>* s, const cx<T>* __restrict__ tw, LD ld)
+// The passes of a radix sequence with a loader on the first and a storer
+// on the last (position-fastest, so a warp stores consecutive points of one
+// line)
+template <typename T, bool INV, int N, int W, int NT, int NS, bool FIRST, typename LD, typename ST, int R0,
+          int... RS>
+__device__ __forceinline__ void fft_ct_chain(cx<T>* s, const cx<T>* __restrict__ tw, LD ld, ST st)
 {
-    fft_pass_ct<T, INV, N, W, NT, R0, 1, LD>(s, tw, ld);
-    fft_ct_passes<T, INV, N, W, NT, R0, RS...>(s, tw);
+    constexpr bool LAST = sizeof...(RS) == 0;
+    if constexpr (FIRST && LAST) fft_pass_ct<T, INV, N, W, NT, R0, NS, LD, ST, true>(s, tw, ld, st);
+    else if constexpr (FIRST) fft_pass_ct<T, INV, N, W, NT, R0, NS, LD, TileSt>(s, tw, ld, TileSt{});
+    else if constexpr (LAST) fft_pass_ct<T, INV, N, W, NT, R0, NS, TileLd, ST, true>(s, tw, TileLd{}, st);
+    else fft_pass_ct<T, INV, N, W, NT, R0, NS>(s, tw);
+    if constexpr (!LAST) fft_ct_chain<T, INV, N, W, NT, NS * R0, false, LD, ST, RS...>(s, tw, ld, st);
 }
 
 // Every pass of a radix sequence, the last one handing its outputs to st
@@ -364,13 +375,15 @@ struct ShapeCT {
     {
         fft_ct_last_st<T, INV, N_, W_, NT_, 1, ST, RS...>(s, tw, st);
     }
-    // the same transform with the first pass reading ld(n, l); the caller
+    // the same transform with the first pass reading ld(n, l) and the last
+    // one handing output n of line l to st(n, l, value); the caller
     // synchronises before (ld's sources ready), the first pass's barrier
-    // separates every ld from the in-place stores
-    template <typename T, bool INV, typename LD>
-    static __device__ __forceinline__ void fft_ld(cx<T>* s, const cx<T>* __restrict__ tw, LD ld)
+    // separates every ld from the in-place stores, and every read of the tile
+    // is done when it returns
+    template <typename T, bool INV, typename LD, typename ST>
+    static __device__ __forceinline__ void fft_ld_st(cx<T>* s, const cx<T>* __restrict__ tw, LD ld, ST st)
     {
-        fft_ct_first_ld<T, INV, N_, W_, NT_, LD, RS...>(s, tw, ld);
+        fft_ct_chain<T, INV, N_, W_, NT_, 1, true, LD, ST, RS...>(s, tw, ld, st);
     }
 };
 

@@ -602,11 +602,11 @@ __global__ void __launch_bounds__(SH::NT) k_xinv_pipe(const cx<T>* __restrict__ 
             const cx<T> O = cmul(D, conj(ldg(tw_n + m)));
             return mk<T>(Ev.x - O.y, Ev.y + O.x);
         };
-        SH::template fft_ld<T, true>(cur, tw_half, zsplit);
-        for (int e = threadIdx.x; e < NC * W; e += NT) {
-            const int l = e / NC, n = e - l * NC;
-            if (line0 + l >= nlines) continue;
-            const cx<T> zv = cur[sidx_ct<T, W>(n, l)];
+        // the last pass hands z_n of line l to the output (x_2n, x_2n+1 are
+        // its real and imaginary parts); a warp writes consecutive points of
+        // one line
+        auto zout = [&](int n, int l, cx<T> zv) {
+            if (line0 + l >= nlines) return;
             const double x0 = (double)zv.x, x1 = (double)zv.y;
             const long o = line_base[l] + 2 * n;
             double u0 = x0, u1 = x1;
@@ -626,7 +626,8 @@ __global__ void __launch_bounds__(SH::NT) k_xinv_pipe(const cx<T>* __restrict__ 
                 acc_u += u0 * u0 + u1 * u1;
                 acc_s += u0 + u1;
             }
-        }
+        };
+        SH::template fft_ld_st<T, true>(cur, tw_half, zsplit, zout);
         __syncthreads();  // cur and the line tables are refilled
         if (GHOST) x_ghosts<UK>(P, U, g, line0, W, nlines, NX);
         cx<T>* tmp = cur;
