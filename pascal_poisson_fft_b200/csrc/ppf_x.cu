@@ -511,9 +511,10 @@ __global__ void __launch_bounds__(SH::NT, 5) k_xinv64(PPF_XINV_PARAMS)
 // x inverse of FP32 spectra, periodic x, compile-time shapes: persistent
 // CTAs walk tiles of W lines; the next tile's half-spectrum rows are copied
 // with cp.async into the second of two raw buffers ([k][line], nc+1 rows)
-// while the current tile is split in place (C2R, pairs (k, nc-k)),
-// transformed and written out -- the output semantics of
-// k_xinv<T, false, ACC, GHOST>.  (FP64 tiles take the non-pipelined kernel:
+// while the current tile is transformed: the C2R split is formed as the
+// first FFT pass loads its inputs, and the last pass hands its outputs to
+// the accumulate and store -- the output semantics of
+// k_xinv<T, false, ACC, GHOST, SH, UK>.  (FP64 tiles take the non-pipelined kernel:
 // two 66 KB buffers at 128 registers leave too few resident CTAs.)
 // --------------------------------------------------------------------------
 template <typename T, bool ACC, bool GHOST, typename SH, int UK = U_P>
@@ -526,7 +527,6 @@ __global__ void __launch_bounds__(SH::NT) k_xinv_pipe(const cx<T>* __restrict__ 
 {
     if (skip && *skip) return;
     constexpr int NC = SH::N, W = SH::W, NT = SH::NT;
-    constexpr int LGW = ct_log2(W);
     constexpr int NR = NC + 1;
     constexpr int ER = NR * W;
     constexpr int NX = 2 * NC;
