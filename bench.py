@@ -46,7 +46,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, nargs=3, default=[512, 512, 512], help="n1m n2m n3m")
-    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true",
+                    help="skip the end-to-end run and the 768x768x384 FP32 run (profiling runs)")
     ap.add_argument("--no-cpu", action="store_true")
     return ap.parse_args()
 
@@ -247,16 +248,17 @@ def run_ours(args, ws, rank, lrank):
     if sweeps is None:
         sweeps = 4
 
-    def timed(plan, out, k):
+    def timed(plan, out, k, inputs=None):
+        fi, d1, d2, d3, x3 = inputs if inputs is not None else (f, dmx1, dmx2, dmx3, dx3)
         for _ in range(args.warmup):
-            plan.solve(f, out, dmx1, dmx2, dmx3, dx3)
+            plan.solve(fi, out, d1, d2, d3, x3)
         if ws > 1:
             torch.distributed.barrier()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(st)
         for _ in range(k):
-            plan.solve(f, out, dmx1, dmx2, dmx3, dx3)
+            plan.solve(fi, out, d1, d2, d3, x3)
         e1.record(st)
         torch.cuda.synchronize()
         return max_over_ranks(e0.elapsed_time(e1) / k, ws, dev)
@@ -335,6 +337,29 @@ def run_ours(args, ws, rank, lrank):
         for q in plans[1:]:
             q.close()
 
+    # the FP32 single-solve throughput run of the same configuration family at
+    # mixed radix 3*2^k (768 = 3*256): 768x768x384, no refinement, its error
+    # against the FP64 solve of the same input reported beside it
+    fp32_run = None
+    if not args.no_e2e and tuple(args.n) == (512, 512, 512):
+        q = W.config3(n1m=768, n2m=768, n3m=384, generate=False)
+        fq = W.config3_field(q, seed=3 + rank, device=dev)
+        qin = (fq, *[t(q.metrics[k]) for k in ("dmx1", "dmx2", "dmx3", "dx3")])
+        Pq = torch.zeros(q.n3m + 2, q.n2m + 2, q.n1m + 2, dtype=torch.float64, device=dev)
+        Rq = torch.zeros_like(Pq)
+        pq64 = ppf.Plan(768, 768, 384, q.L1, q.L2, *q.pbc, precision=ppf.PPF_FP64)
+        pq64.solve(*qin[:1], Rq, *qin[1:])
+        pq64.close()
+        pq32 = ppf.Plan(768, 768, 384, q.L1, q.L2, *q.pbc, precision=ppf.PPF_FP32)
+        ms32 = timed(pq32, Pq, args.steps, qin)
+        rel32 = float(torch.linalg.vector_norm(Pq - Rq) / torch.linalg.vector_norm(Rq))
+        pq32.close()
+        fp32_run = {"workload": "768x768x384 Poisson, periodic x,y / Neumann z, tanh z beta=1.5, FP32 single solve "
+                                "(radix 3*2^k, no refinement)",
+                    "value": ws * 1000.0 / ms32, "unit": "solves/s", "ms_per_step": ms32,
+                    "rel_l2_vs_fp64": rel32}
+        del Pq, Rq, qin, fq
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         try:
@@ -369,6 +394,7 @@ def run_ours(args, ws, rank, lrank):
             "gpu_launches": int(round(launches_per_solve * args.steps)),
             "clocks": clk,
             "e2e": e2e,
+            "fp32_768x768x384": fp32_run,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
