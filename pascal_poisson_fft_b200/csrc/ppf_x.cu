@@ -718,7 +718,7 @@ cudaError_t launch_xinv(bool dct, const void* in, long in_pitch, double* P, floa
     if (ukind != U_P && (sizeof(T) != 4 || !U || !stencil_ghosts || accumulate != (ukind == U_ACC)))
         return cudaErrorInvalidValue;
     cudaError_t err = cudaSuccess;
-    with_shape<T>(sch, [&](auto sh) {
+    with_shape<T, true>(sch, [&](auto sh) {
         using SH = decltype(sh);
         int W, threads;
         shape_geom<T, SH>(sch, W, threads);
@@ -794,7 +794,7 @@ template <typename T>
 long xinv_blocks(const Geom& g, const FftSched& sch)
 {
     long blocks = 0;
-    with_shape<T>(sch, [&](auto sh) {
+    with_shape<T, true>(sch, [&](auto sh) {
         using SH = decltype(sh);
         int W, threads;
         shape_geom<T, SH>(sch, W, threads);

@@ -46,8 +46,10 @@ inline int pick_w(int n, int& threads)
 
 // Compile-time shapes of the common lengths: W lines, NT threads (16 FP32
 // or 8 FP64 elements per thread), radix sequence.  Other lengths use the
-// run-time engine.
-template <typename T, typename F>
+// run-time engine.  XINV: the shape of the x inverse, whose FP32 384-point
+// lines run faster with the radix-3 pass last (the other transforms with it
+// first); the tile width is the same either way.
+template <typename T, bool XINV = false, typename F>
 void with_shape(const FftSched& sch, F&& f)
 {
     const int n = sch.n;
@@ -69,9 +71,12 @@ void with_shape(const FftSched& sch, F&& f)
             case 64:  f(ShapeCT<64, 64, 256, 8, 8>{}); return;
             case 128: f(ShapeCT<128, 32, 256, 8, 4, 4>{}); return;
             case 256: f(ShapeCT<256, 8, 256, 8, 8, 4>{}); return;
-            case 384: f(ShapeCT<384, 16, 384, 8, 4, 4, 3>{}); return;
+            case 384:
+                if constexpr (XINV) f(ShapeCT<384, 8, 384, 8, 4, 4, 3>{});
+                else f(ShapeCT<384, 8, 384, 3, 8, 4, 4>{});
+                return;
             case 512: f(ShapeCT<512, 16, 512, 8, 8, 8>{}); return;
-            case 768: f(ShapeCT<768, 8, 384, 8, 8, 4, 3>{}); return;
+            case 768: f(ShapeCT<768, 8, 384, 3, 8, 8, 4>{}); return;
             default: break;
         }
     }
