@@ -518,7 +518,7 @@ __global__ void __launch_bounds__(SH::NT, 5) k_xinv64(PPF_XINV_PARAMS)
 // two 66 KB buffers at 128 registers leave too few resident CTAs.)
 // --------------------------------------------------------------------------
 template <typename T, bool ACC, bool GHOST, typename SH, int UK = U_P>
-__global__ void __launch_bounds__(SH::NT, SH::N == 384 ? 2 : 0) k_xinv_pipe(const cx<T>* __restrict__ in, long in_pitch,
+__global__ void __launch_bounds__(SH::NT, (SH::N == 384 || SH::N <= 128) ? 2 : 0) k_xinv_pipe(const cx<T>* __restrict__ in, long in_pitch,
                                                      double* __restrict__ P, float* __restrict__ U, Geom g,
                                                      double* __restrict__ partials,
                                                      const double* __restrict__ mean_prev,
