@@ -131,17 +131,26 @@ def measured_hbm_peak():
 
 
 def stage_bytes(p, prec_bytes, sweeps):
-    """Algorithmic bytes per stage, summed over one solve (periodic x and y).
+    """Algorithmic bytes per stage, summed over one solve.
 
     Every pass reads and writes one spectral field per y and z stage; the x
-    forward reads f (FP64) and writes the spectrum, the x inverse reads the
-    spectrum and writes the iterate.  With refinement sweeps the first
+    forward reads f (FP64) and writes the x spectrum A, the x inverse reads A
+    and writes the iterate.  A is (n1m/2+1) complex values per (y, z) line for
+    periodic x and n1m reals for a DCT in x; the y spectrum B is complex for
+    periodic x or y and real for DCT in both.  With refinement sweeps the first
     iterate is an FP32 ghosted field (4 bytes a cell, written by the first
     pass, read by the first sweep's residual and accumulate); later sweeps
     read and write the FP64 iterate (8 bytes a cell)."""
     n1, n2, n3 = p.n1m, p.n2m, p.n3m
     N = n1 * n2 * n3
-    spec = (n1 // 2 + 1) * n2 * n3 * 2 * prec_bytes  # one half-spectrum field
+    px, py = bool(p.pbc[0]), bool(p.pbc[1])
+    spec_a = (n1 // 2 + 1) * n2 * n3 * 2 * prec_bytes if px else N * prec_bytes
+    if px:
+        spec_b = spec_a
+    elif py:
+        spec_b = n1 * (n2 // 2 + 1) * n3 * 2 * prec_bytes
+    else:
+        spec_b = N * prec_bytes
     runs = 1 + sweeps
     if sweeps == 0 or prec_bytes == 8:
         u_read, u_rw = 0, 8 * N
@@ -149,12 +158,22 @@ def stage_bytes(p, prec_bytes, sweeps):
         u_read = 4 * N + (sweeps - 1) * 8 * N           # residual reads of the iterate
         u_rw = 4 * N + (4 * N + 8 * N) + (sweeps - 1) * 16 * N   # x-inverse writes + accumulate reads
     return {
-        "x-forward": runs * (8 * N + spec) + u_read,
-        "y-forward": runs * 2 * spec,
-        "tdma-z": runs * 2 * spec,
-        "y-inverse": runs * 2 * spec,
-        "x-inverse": runs * spec + u_rw,
+        "x-forward": runs * (8 * N + spec_a) + u_read,
+        "y-forward": runs * (spec_a + spec_b),
+        "tdma-z": runs * 2 * spec_b,
+        "y-inverse": runs * (spec_a + spec_b),
+        "x-inverse": runs * spec_a + u_rw,
     }
+
+
+def stage_report(stages, sb, k, peak):
+    """Per-stage ms per solve, achieved GB/s and fraction of the HBM peak."""
+    out = {}
+    for name, nbytes in sb.items():
+        ms = stages[name][0] / k
+        gbs = nbytes / (ms * 1e-3) / 1e9 if ms > 0 else None
+        out[name] = {"ms": ms, "gbs": gbs, "frac": gbs / peak if gbs else None}
+    return out
 
 
 def load_traffic(kernel: str):
@@ -168,12 +187,39 @@ def load_traffic(kernel: str):
         return None
 
 
-def cpu_baseline(p, threads):
+def cpu_baseline(p, threads, keep=False):
+    """Seconds of one oracle solve of p (and its output when keep)."""
     from oracle import oracle as O
     m = p.metrics
     t0 = time.perf_counter()
-    O.poisson_solve(p.f, p.L1, p.L2, p.pbc, m["dmx1"], m["dmx2"], m["dmx3"], m["dx3"], nthreads=threads)
-    return time.perf_counter() - t0
+    out = O.poisson_solve(p.f, p.L1, p.L2, p.pbc, m["dmx1"], m["dmx2"], m["dmx3"], m["dx3"], nthreads=threads)
+    sec = time.perf_counter() - t0
+    return (sec, out) if keep else sec
+
+
+def cpu_stage_seconds():
+    """The last oracle solve's stages under the reference's timer labels
+    (01_Fortran/examples/main.f90:65-78)."""
+    from oracle import oracle as O
+    st = O.last_stage_seconds()
+    if st is None:
+        return None
+    return {"build TDMA + FFT forward": st["setup"] + st["fft-forward"], "TDMA": st["tdma-z"],
+            "FFT backward": st["fft-inverse"], "update solution": st["update-solution"]}
+
+
+def scipy_fft_stage(f, workers):
+    """Seconds of the x/y transform stages of one periodic solve with
+    scipy.fft (pocketfft): real FFT along x, complex FFT along y, and back."""
+    import scipy.fft as sf
+    t0 = time.perf_counter()
+    c = sf.rfft(f, axis=2, workers=workers)
+    c = sf.fft(c, axis=1, workers=workers, overwrite_x=True)
+    t1 = time.perf_counter()
+    c = sf.ifft(c, axis=1, workers=workers, overwrite_x=True)
+    sf.irfft(c, n=f.shape[2], axis=2, workers=workers)
+    t2 = time.perf_counter()
+    return t1 - t0, t2 - t1
 
 
 def run_reference(args, ws, rank):
@@ -208,6 +254,108 @@ def run_reference(args, ws, rank):
                              "sample": sample},
             "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def _device_time(fn, k, warm, stream):
+    """ms per call of fn (CUDA events on `stream`, after `warm` calls)."""
+    import torch
+    for _ in range(warm):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(k):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / k
+
+
+def other_configs(args, dev, peak):
+    """The other workloads of the configuration set, one GPU each, each timed
+    with CUDA events and checked against its reference answer:
+    c1 64^3 FP64 (periodic x,y), c2 256^3 FP64 DCT x,y with tanh z (beta 2),
+    c4 96 uneven problems in one graph launch (FP64 and mixed), c5 the
+    256x256x128 adjoint (FP64 and mixed)."""
+    import torch
+    import pascal_poisson_fft_b200 as ppf
+    from oracle import oracle as O
+    from pascal_poisson_fft_b200 import workloads as W
+    st = torch.cuda.current_stream()
+    t = lambda a: torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float64, device=dev)
+    k = max(5, min(args.steps, 20))
+    out = {}
+
+    def plain(p, name):
+        m = p.metrics
+        mm = [t(m[q]) for q in ("dmx1", "dmx2", "dmx3", "dx3")]
+        fd = t(p.f)
+        P = torch.zeros(p.n3m + 2, p.n2m + 2, p.n1m + 2, dtype=torch.float64, device=dev)
+        plan = ppf.Plan(p.n1m, p.n2m, p.n3m, p.L1, p.L2, *p.pbc, precision=ppf.PPF_FP64)
+        ms = _device_time(lambda: plan.solve(fd, P, *mm), k, 3, st)
+        plan.stage_timing(True)
+        for _ in range(3):
+            plan.solve(fd, P, *mm)
+        stg = plan.stage_times()
+        plan.stage_timing(False)
+        R = O.poisson_solve(p.f, p.L1, p.L2, p.pbc, m["dmx1"], m["dmx2"], m["dmx3"], m["dx3"])
+        rel = float(np.linalg.norm(P.cpu().numpy() - R) / np.linalg.norm(R))
+        sb = stage_bytes(p, 8, 0)
+        tot = sum(sb.values())
+        plan.close()
+        return {"workload": name, "value": 1000.0 / ms, "unit": "solves/s", "ms_per_step": ms,
+                "mcells_s": p.n1m * p.n2m * p.n3m / ms / 1e3, "gbs_alg": tot / (ms * 1e-3) / 1e9,
+                "hbm_frac": tot / (ms * 1e-3) / 1e9 / peak, "rel_l2_vs_oracle": rel,
+                "stages": stage_report(stg, sb, 3, peak)}
+
+    out["c1"] = plain(W.config1(), "64^3 FP64, periodic x,y, Neumann z, uniform")
+    out["c2"] = plain(W.config2(), "256^3 FP64, DCT x,y, Neumann z, tanh z beta=2")
+
+    # c4: 96 uneven problems, one graph launch per batch solve
+    probs = W.config4(device=dev)
+    cells = sum(p.n1m * p.n2m * p.n3m for p in probs)
+    fs = [p.f for p in probs]
+    ms_ = [[t(p.metrics[q]) for p in probs] for q in ("dmx1", "dmx2", "dmx3", "dx3")]
+    res = {}
+    outs = {}
+    for prec, name, sw in ((ppf.PPF_FP64, "fp64", 0), (ppf.PPF_MIXED, "mixed", 2)):
+        t0 = time.perf_counter()
+        b = ppf.Batch([dict(n1m=p.n1m, n2m=p.n2m, n3m=p.n3m, L1=p.L1, L2=p.L2, pbc=p.pbc, precision=prec,
+                            max_sweeps=sw) for p in probs], autotune=True)
+        t_create = time.perf_counter() - t0
+        Ps = [torch.zeros(p.n3m + 2, p.n2m + 2, p.n1m + 2, dtype=torch.float64, device=dev) for p in probs]
+        ms = _device_time(lambda: b.solve(fs, Ps, *ms_), k, 3, st)
+        res[name] = {"ms_per_batch": ms, "gcells_s": cells / ms / 1e6, "create_s": t_create}
+        outs[name] = Ps
+        b.close()
+    worst = max(float(torch.linalg.vector_norm(a - c) / torch.linalg.vector_norm(c))
+                for a, c in zip(outs["mixed"], outs["fp64"]))
+    res["mixed"]["max_rel_l2_vs_fp64"] = worst
+    out["c4"] = {"workload": f"96 uneven problems ({cells / 1e6:.0f} Mcells), one graph launch", **res}
+    del outs, fs, probs
+
+    # c5: adjoint at 256x256x128 (transpose solve + z-metric gradient)
+    p, _ = W.config5()
+    m = p.metrics
+    mm = [t(m[q]) for q in ("dmx1", "dmx2", "dmx3", "dx3")]
+    fd = t(p.f)
+    res = {}
+    for prec, name in ((ppf.PPF_FP64, "fp64"), (ppf.PPF_MIXED, "mixed")):
+        plan = ppf.Plan(p.n1m, p.n2m, p.n3m, p.L1, p.L2, *p.pbc, precision=prec, max_sweeps=3)
+        u = torch.zeros(plan.gshape, dtype=torch.float64, device=dev)
+        plan.solve(fd, u, *mm)
+        df = torch.empty(plan.shape, dtype=torch.float64, device=dev)
+        gx = torch.empty(p.n3m + 2, dtype=torch.float64, device=dev)
+        gm = torch.empty(p.n3m + 2, dtype=torch.float64, device=dev)
+        ms_f = _device_time(lambda: plan.solve(fd, u, *mm), k, 3, st)
+        ms_a = _device_time(lambda: plan.solve_adjoint(fd, df, *mm, u=u, ddx3=gx, ddmx3=gm), k, 3, st)
+        res[name] = {"forward_ms": ms_f, "adjoint_ms": ms_a}
+        plan.close()
+    n1, n2, n3 = p.n1m, p.n2m, p.n3m
+    res["recompute_bytes"] = (n1 + 2) * (n2 + 2) * (n3 + 2) * 8
+    res["store_bytes"] = (n1 // 2 + 1) * n2 * n3 * 16
+    out["c5"] = {"workload": "256x256x128 adjoint (dJ/df and dJ/d dx3, dmx3), periodic x,y, tanh z beta=2", **res}
+    return out
 
 
 def run_ours(args, ws, rank, lrank):
@@ -360,18 +508,44 @@ def run_ours(args, ws, rank, lrank):
                     "rel_l2_vs_fp64": rel32}
         del Pq, Rq, qin, fq
 
-    cpu = None
+    # the CPU baseline (the oracle on all host cores) on the same right-hand
+    # side; its output also pins the headline results: rel-L2 of the FP64 and
+    # of the mixed 512^3 solve against the FP64 oracle
+    cpu, vs_oracle = None, {}
     if rank == 0 and ws == 1 and not args.no_cpu:
         try:
             pc = W.config3(n1m=n1, n2m=n2, n3m=n3, generate=False)
             pc.f = f.cpu().numpy()
             threads = os.cpu_count() or 1
-            sec = cpu_baseline(pc, threads)
+            sec, R = cpu_baseline(pc, threads, keep=True)
+            stages_cpu = cpu_stage_seconds()
+            nrm = float(np.linalg.norm(R))
+            vs_oracle = {"mixed": float(np.linalg.norm(P.cpu().numpy() - R) / nrm),
+                         "fp64": float(np.linalg.norm(P64.cpu().numpy() - R) / nrm)}
+            del R
+            # one host thread, on a z-slab sample of the same workload (the
+            # solve's cost is linear in the z rows), scaled to a whole solve
+            nz1 = min(n3, 64)
+            p1 = W.config3(n1m=n1, n2m=n2, n3m=nz1, generate=False)
+            p1.f = np.ascontiguousarray(pc.f[:nz1])
+            sec1 = cpu_baseline(p1, 1) * (n3 / nz1)
+            fwd, inv = scipy_fft_stage(pc.f, threads)
             cpu = {"value": 1.0 / sec, "unit": "solves/s", "cores": threads, "kind": "port",
-                   "sample": f"one full {n1}x{n2}x{n3} FP64 solve of the same right-hand side"}
+                   "sample": f"one full {n1}x{n2}x{n3} FP64 solve of the same right-hand side",
+                   "stage_s": stages_cpu,
+                   "single_thread": {"value": 1.0 / sec1, "unit": "solves/s", "cores": 1,
+                                     "sample": f"{n1}x{n2}x{nz1} z-slab of the workload, time scaled by {n3}/{nz1}"},
+                   "scipy_fft_stage_s": {"forward x+y": fwd, "inverse y+x": inv, "workers": threads,
+                                         "oracle_forward": stages_cpu["build TDMA + FFT forward"] if stages_cpu else None,
+                                         "oracle_inverse": stages_cpu["FFT backward"] if stages_cpu else None}}
+            del pc
         except Exception as exc:  # the baseline is reported, never the product
             cpu = {"value": None, "unit": "solves/s", "cores": os.cpu_count(), "kind": "port",
                    "sample": f"failed: {exc}"}
+
+    configs = None
+    if rank == 0 and ws == 1 and not args.no_e2e and tuple(args.n) == (512, 512, 512):
+        configs = other_configs(args, dev, peak)
 
     if rank == 0:
         line = {
@@ -382,12 +556,16 @@ def run_ours(args, ws, rank, lrank):
             "config": {"workload": f"{n1}x{n2}x{n3} Poisson, periodic x,y / Neumann z, tanh z beta=1.5, "
                                    f"mixed FP32+FP64 refine ({sweeps} sweeps)",
                        "grid": [n1, n2, n3], "sweeps": sweeps, "rel_l2_vs_fp64": rel,
+                       "rel_l2_vs_oracle": vs_oracle.get("mixed"),
                        "l2_policy": "inputs larger than L2 (1 GiB FP64 field per step)",
                        "problems_per_gpu": 1},
             "fp64_plain": {"value": ws * 1000.0 / ms_fp64, "unit": "solves/s", "ms_per_step": ms_fp64,
-                           "stage_ms_per_solve": {k: v[0] / kst for k, v in stages64.items()}},
+                           "rel_l2_vs_oracle": vs_oracle.get("fp64"),
+                           "stage_ms_per_solve": {k: v[0] / kst for k, v in stages64.items()},
+                           "stages": stage_report(stages64, stage_bytes(p, 8, 0), kst, peak)},
             "mixed_over_fp64": ms_fp64 / ms_mixed,
             "stage_ms_per_solve": {k: v[0] / kst for k, v in stages.items()},
+            "stages": stage_report(stages, sb, kst, peak),
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
                          "bytes_per_launch": dom_bytes_per_launch, "traffic": load_traffic(dom)},
@@ -396,6 +574,7 @@ def run_ours(args, ws, rank, lrank):
             "e2e": e2e,
             "fp32_768x768x384": fp32_run,
             "cpu_baseline": cpu,
+            "configs": configs,
         }
         print(json.dumps(line), flush=True)
     if ws > 1:

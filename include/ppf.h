@@ -228,7 +228,9 @@ PPF_API int ppf_slab_ghosts(ppf_plan *plan, double *p_d, const double *dmx1_d, c
  * GPU loading the library holds until the process exits; grids whose work
  * memory does not fit (about 128^3 cells) are rejected with
  * PPF_ERR_UNSUPPORTED and a message naming the bytes needed.  The first call
- * on a device looks up the array's device address; make that first call
+ * on a device looks up the array's device address and uploads the grid's
+ * wavenumber and twiddle tables (a few KB, cached per CUDA context and grid;
+ * again after a device reset or a change of grid); make that first call
  * before any stream capture.  All calls on a device share the array and it
  * keeps the last call's contents: calls whose kernels overlap on the GPU
  * (different streams, or different host threads without ordering) race on

@@ -52,6 +52,8 @@ def lib():
             [_dp, _dp, _dp, _dp, _dp, _dp, ctypes.c_int, ctypes.c_int]
         L.ora_poisson_solve.restype = ctypes.c_int
         L.ora_fill_ghosts.argtypes = [ctypes.c_int] * 6 + [_dp, _dp, _dp, _dp]
+        L.ora_last_stage_seconds.argtypes = [_dp]
+        L.ora_last_stage_seconds.restype = ctypes.c_int
         L.ora_residual.argtypes = [ctypes.c_int] * 3 + [ctypes.c_double] * 2 + [ctypes.c_int] * 2 + \
             [_dp, _dp, _dp, _dp, _dp]
         _LIB = L
@@ -118,6 +120,16 @@ def poisson_solve(f: np.ndarray, L1: float, L2: float, pbc, dmx1, dmx2, dmx3, dx
     if rc != 0:
         raise ValueError(f"ora_poisson_solve rejected the problem (rc={rc})")
     return P
+
+
+def last_stage_seconds():
+    """Per-stage seconds of the last poisson_solve: setup, forward transforms,
+    z solves, inverse transforms, mean removal + ghosts (None if incomplete)."""
+    out = np.zeros(5)
+    n = lib().ora_last_stage_seconds(_ptr(out))
+    if n != 6:
+        return None
+    return dict(zip(("setup", "fft-forward", "tdma-z", "fft-inverse", "update-solution"), out.tolist()))
 
 
 def fill_ghosts(P: np.ndarray, pbc, dmx1, dmx2, dmx3) -> None:

@@ -499,6 +499,33 @@ static int nthreads_set(int nt)
 #define OMP_PARALLEL
 #endif
 
+/* Wall-clock stamps of the last ora_poisson_solve: start, then before each of
+ * its parallel regions (forward transforms, z solves, inverse transforms),
+ * before the mean removal and at the end.  ora_last_stage_seconds() turns
+ * them into the reference's timer stages (01_Fortran/examples/main.f90:65-78:
+ * build TDMA + transforms, TDMA, update solution). */
+static double g_stamps[16];
+static int g_nstamp = 0;
+#ifdef _OPENMP
+#define ORA_STAMP() do { if (g_nstamp < 16) g_stamps[g_nstamp++] = omp_get_wtime(); } while (0)
+#else
+#define ORA_STAMP() do { } while (0)
+#endif
+
+/* Seconds of the last solve per stage: [0] set-up (wavenumbers, z
+ * coefficients), [1] forward x/y transforms, [2] z tridiagonal solves,
+ * [3] inverse y/x transforms, [4] mean removal and ghost cells.  Returns the
+ * number of stamps taken (6 when every stage was seen). */
+int ora_last_stage_seconds(double *out)
+{
+    for (int i = 0; i < 5; ++i) out[i] = 0.0;
+    if (g_nstamp != 6) return g_nstamp;
+    /* stamps: start, before the forward transforms, the z solves, the inverse
+       transforms, the mean removal, and the end */
+    for (int i = 0; i < 5; ++i) out[i] = g_stamps[i + 1] - g_stamps[i];
+    return g_nstamp;
+}
+
 int ora_poisson_solve(int n1m, int n2m, int n3m, double L1, double L2,
                       int pbc1, int pbc2, int pbc3,
                       const double *f, double *P,
@@ -508,6 +535,8 @@ int ora_poisson_solve(int n1m, int n2m, int n3m, double L1, double L2,
 {
     if (n1m < 2 || n2m < 2 || n3m < 3 || (n1m & 1) || (n2m & 1)) return -1;
     nthreads_set(nthreads);
+    g_nstamp = 0;
+    ORA_STAMP();
     const long nx = n1m, ny = n2m, nz = n3m;
     const long ncell = nx * ny * nz;
     double *dxk2 = (double *)malloc(sizeof(double) * nx);
@@ -523,6 +552,7 @@ int ora_poisson_solve(int n1m, int n2m, int n3m, double L1, double L2,
     if (!pbc1 && !pbc2) {
         /* ---- N-N : real DCT in x, real DCT in y, real TDMA ---- */
         double *X = (double *)malloc(sizeof(double) * ncell);  /* (i,j,k) */
+        ORA_STAMP();
         OMP_PARALLEL
         {
             axis_ws wx, wy;
@@ -542,6 +572,7 @@ int ora_poisson_solve(int n1m, int n2m, int n3m, double L1, double L2,
         }
         /* TDMA-z (cuda_Poisson_TDMA_z_real :1121-1170): systems (i,j), i fastest.
            Solved per j-row block of n1m systems (independent systems). */
+        ORA_STAMP();
         OMP_PARALLEL
         {
             double *lam = (double *)malloc(sizeof(double) * nx);
@@ -557,6 +588,7 @@ int ora_poisson_solve(int n1m, int n2m, int n3m, double L1, double L2,
             }
             free(lam); free(d);
         }
+        ORA_STAMP();
         OMP_PARALLEL
         {
             axis_ws wx, wy;
@@ -583,6 +615,7 @@ int ora_poisson_solve(int n1m, int n2m, int n3m, double L1, double L2,
         const long hy = ny / 2 + 1;
         double *X = (double *)malloc(sizeof(double) * ncell);
         cd *C = (cd *)malloc(sizeof(cd) * nx * hy * nz);      /* (i, jy, k) */
+        ORA_STAMP();
         OMP_PARALLEL
         {
             axis_ws wx, wy;
@@ -597,6 +630,7 @@ int ora_poisson_solve(int n1m, int n2m, int n3m, double L1, double L2,
             }
             axis_ws_free(&wx); axis_ws_free(&wy);
         }
+        ORA_STAMP();
         OMP_PARALLEL
         {
             double *lam = (double *)malloc(sizeof(double) * nx);
@@ -620,6 +654,7 @@ int ora_poisson_solve(int n1m, int n2m, int n3m, double L1, double L2,
             }
             free(lam); free(dr); free(di);
         }
+        ORA_STAMP();
         OMP_PARALLEL
         {
             axis_ws wx, wy;
@@ -645,6 +680,7 @@ int ora_poisson_solve(int n1m, int n2m, int n3m, double L1, double L2,
         const long hx = nx / 2 + 1;
         double *Y = (double *)malloc(sizeof(double) * ncell);  /* (i,j,k) */
         cd *C = (cd *)malloc(sizeof(cd) * hx * ny * nz);      /* (ix, j, k) */
+        ORA_STAMP();
         OMP_PARALLEL
         {
             axis_ws wx, wy;
@@ -659,6 +695,7 @@ int ora_poisson_solve(int n1m, int n2m, int n3m, double L1, double L2,
                 r2c_line(&wx, Y + jk * nx, 1, C + jk * hx, 1);
             axis_ws_free(&wx); axis_ws_free(&wy);
         }
+        ORA_STAMP();
         OMP_PARALLEL
         {
             double *lam = (double *)malloc(sizeof(double) * ny);
@@ -682,6 +719,7 @@ int ora_poisson_solve(int n1m, int n2m, int n3m, double L1, double L2,
             }
             free(lam); free(dr); free(di);
         }
+        ORA_STAMP();
         OMP_PARALLEL
         {
             axis_ws wx, wy;
@@ -706,6 +744,7 @@ int ora_poisson_solve(int n1m, int n2m, int n3m, double L1, double L2,
         /* ---- P-P : R2C in x, C2C in y, complex TDMA ---- */
         const long hx = nx / 2 + 1;
         cd *C = (cd *)malloc(sizeof(cd) * hx * ny * nz);      /* (ix, j, k) */
+        ORA_STAMP();
         OMP_PARALLEL
         {
             axis_ws wx, wy;
@@ -720,6 +759,7 @@ int ora_poisson_solve(int n1m, int n2m, int n3m, double L1, double L2,
             }
             axis_ws_free(&wx); axis_ws_free(&wy);
         }
+        ORA_STAMP();
         OMP_PARALLEL
         {
             double *lam = (double *)malloc(sizeof(double) * ny);
@@ -747,6 +787,7 @@ int ora_poisson_solve(int n1m, int n2m, int n3m, double L1, double L2,
             }
             free(lam); free(dr); free(di);
         }
+        ORA_STAMP();
         OMP_PARALLEL
         {
             axis_ws wx, wy;
@@ -769,6 +810,7 @@ int ora_poisson_solve(int n1m, int n2m, int n3m, double L1, double L2,
         free(C);
     }
 
+    ORA_STAMP();
     /* cuda_Poisson_average_elimination :628-664 (arithmetic mean) */
     double aver = 0.0;
     for (long q = 0; q < ncell; ++q) aver += tmp[q];
@@ -784,6 +826,7 @@ int ora_poisson_solve(int n1m, int n2m, int n3m, double L1, double L2,
     }
     ora_fill_ghosts(n1m, n2m, n3m, pbc1, pbc2, pbc3, P, dmx1, dmx2, dmx3);
 
+    ORA_STAMP();
     free(tmp); free(dxk2); free(dyk2); free(am); free(ap);
     return rc;
 }

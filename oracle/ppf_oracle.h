@@ -76,6 +76,12 @@ void ora_fill_ghosts(int n1m, int n2m, int n3m, int pbc1, int pbc2, int pbc3,
  * spacing L/N; finite-volume z stencil with am=1/(dx3_k dmx3_k),
  * ap=1/(dx3_k dmx3_{k+1}), am_1 = ap_n3m = 0).  u is read from the interior
  * of the ghosted array P.  No reference counterpart (a residual check). */
+/* Seconds of the last ora_poisson_solve per stage: set-up, forward
+ * transforms, z solves, inverse transforms, mean removal + ghosts (the
+ * reference's timer stages, 01_Fortran/examples/main.f90:65-78).  Returns
+ * the number of stamps (6 = complete). */
+int ora_last_stage_seconds(double *out);
+
 void ora_residual(int n1m, int n2m, int n3m, double L1, double L2,
                   int pbc1, int pbc2, const double *f, const double *P,
                   const double *dmx3, const double *dx3, double *r);

@@ -3,6 +3,7 @@
 #include "ppf_kernels.cuh"
 #include "ppf_xy_common.cuh"
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -917,10 +918,42 @@ constexpr int NA_MAXDEV = 64;
 constexpr size_t NA_STAGE = 32768;  // host staging of the tables (doubles)
 
 struct NoallocDev {
-    unsigned char* base = nullptr;  // device address of g_noalloc_scratch on this device
+    unsigned char* base = nullptr;  // device address of g_noalloc_scratch in context `ctx`
+    unsigned long long ctx = 0;     // id of the CUDA context `base` and the tables belong to
     bool tables = false;            // tables of `last` are in the array
     ppf_desc last{};
 };
+
+// Unique id of the calling thread's current CUDA context (0 if the driver
+// cannot tell).  A device reset or a new primary context gets a new id, and
+// the static array is then a new allocation whose contents (the cached
+// tables) are gone and whose address may differ, so the cache is keyed on it.
+unsigned long long current_context_id()
+{
+    using GetCurrent = CUresult (*)(CUcontext*);
+    using GetId = CUresult (*)(CUcontext, unsigned long long*);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static bool looked_up = false;
+    if (!looked_up) {
+        looked_up = true;
+        cudaDriverEntryPointQueryResult q;
+        void* fn = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<GetCurrent>(fn);
+        fn = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<GetId>(fn);
+    }
+    if (!get_current || !get_id) return 0;
+    CUcontext c = nullptr;
+    unsigned long long id = 0;
+    if (get_current(&c) != CUDA_SUCCESS || !c) return 0;
+    if (get_id(c, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
 
 std::mutex g_na_mu;
 NoallocDev g_na[NA_MAXDEV];
@@ -958,13 +991,17 @@ extern "C" int ppf_solve_noalloc(const ppf_desc* desc, const double* f_d, double
     PPF_CK(cudaGetDevice(&dev));
     if (dev < 0 || dev >= NA_MAXDEV) return fail(PPF_ERR_UNSUPPORTED, "device index %d out of range", dev);
     NoallocDev& nd = g_na[dev];
-    if (!nd.base) {
-        // first call on this device: the device address of the array (the
-        // host-side symbol is not a device address)
+    const unsigned long long ctx = current_context_id();   // 0 while no context is current yet
+    if (!nd.base || ctx == 0 || ctx != nd.ctx) {
+        // first call on this device, or in a new context after a device
+        // reset: the device address of the array (the host-side symbol is
+        // not a device address; the lookup also creates the device's primary
+        // context if none is current) and the tables must be uploaded again
         void* ptr = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
         if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
         nd.base = static_cast<unsigned char*>(ptr);
+        nd.ctx = current_context_id();
         nd.tables = false;
     }
 

@@ -129,21 +129,54 @@ def slab_rows(n3m: int, nranks: int, rank: int):
     return z0, rows
 
 
+def halo_ops(rank, nranks, periodic):
+    """The point-to-point messages of one ghost-plane exchange, in posting
+    order: ("send", plane, peer) / ("recv", plane, peer), planes indexed in
+    the ghosted layout (0 and n+1 are the ghost planes, 1 and n the first
+    and last interior ones; n is passed symbolically as -1 and n+1 as -2).
+
+    Messages between one pair of ranks are matched in posting order (NCCL
+    ignores tags), so the order is chosen to be right even when both
+    neighbours are the same rank (two ranks with periodic z): sends go out as
+    (first plane -> lower neighbour, last plane -> upper neighbour) and
+    receives are posted as (upper ghost <- upper neighbour, lower ghost <-
+    lower neighbour).  The k-th plane a rank sends to a peer then lands in
+    the k-th plane that peer receives from it: a rank's first plane fills
+    the upper ghost of the rank below it, its last plane the lower ghost of
+    the rank above it."""
+    lo = rank - 1 if rank > 0 else (nranks - 1 if periodic else None)
+    hi = rank + 1 if rank < nranks - 1 else (0 if periodic else None)
+    ops = []
+    if lo is not None:
+        ops.append(("send", 1, lo))
+    if hi is not None:
+        ops.append(("send", -1, hi))
+    if hi is not None:
+        ops.append(("recv", -2, hi))
+    if lo is not None:
+        ops.append(("recv", 0, lo))
+    return ops
+
+
 def halo_exchange(P, rank, nranks, periodic, group=None):
     """Ghost planes between slabs: this rank's first and last interior z
     planes to the neighbours' upper and lower ghost planes (whole planes of
-    the ghosted layout), wrapping around when z is periodic."""
+    the ghosted layout), wrapping around when z is periodic.  A single
+    periodic rank copies its own planes."""
     import torch.distributed as dist
     n = P.shape[0] - 2
+    if nranks == 1:
+        if periodic:
+            P[0].copy_(P[n])
+            P[n + 1].copy_(P[1])
+        return
+    idx = {0: 0, 1: 1, -1: n, -2: n + 1}
     ops = []
-    lo = rank - 1 if rank > 0 else (nranks - 1 if periodic else None)
-    hi = rank + 1 if rank < nranks - 1 else (0 if periodic else None)
-    if lo is not None:
-        ops.append(dist.P2POp(dist.isend, P[1].contiguous(), lo, group))
-        ops.append(dist.P2POp(dist.irecv, P[0], lo, group))
-    if hi is not None:
-        ops.append(dist.P2POp(dist.isend, P[n].contiguous(), hi, group))
-        ops.append(dist.P2POp(dist.irecv, P[n + 1], hi, group))
+    for kind, plane, peer in halo_ops(rank, nranks, periodic):
+        if kind == "send":
+            ops.append(dist.P2POp(dist.isend, P[idx[plane]].contiguous(), peer, group))
+        else:
+            ops.append(dist.P2POp(dist.irecv, P[idx[plane]], peer, group))
     if ops:
         for req in dist.batch_isend_irecv(ops):
             req.wait()

@@ -130,7 +130,7 @@ def _halo_worker(rank, ws, port, periodic, out):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("ws,periodic", [(2, False), (3, True), (3, False)])
+@pytest.mark.parametrize("ws,periodic", [(2, False), (2, True), (3, True), (3, False), (1, True)])
 def test_gloo_halo_exchange(ws, periodic):
     import torch.multiprocessing as mp
     ctx = mp.get_context("spawn")

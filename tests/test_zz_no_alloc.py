@@ -3,10 +3,14 @@
 Some callers cannot allocate device memory when they solve: a flow solver
 that reserved its whole device budget at start-up, or an application whose
 device memory belongs to another framework.  ppf_solve_noalloc serves them
-from one static device array; these tests call it through the C ABI twice
-in a row (different grids, so the second call also replaces the cached
-tables) and compare each result with ppf_plan_create + ppf_solve.  This file
-is collected last so a failure here never hides the other tests.
+from one static device array.  These tests call it through the C ABI on a
+sequence of grids -- first, second, first, first -- so the table upload,
+the cached-table path (same grid again) and the return to an earlier grid
+after another one are all exercised.  ppf_solve_noalloc runs the same
+kernels on the same inputs as ppf_plan_create + ppf_solve, so every result
+must equal the plan solve's bit for bit, and the FP64 oracle within the
+FP64 tolerance.  This file is collected last so a failure here never hides
+the other tests.
 """
 import ctypes
 
@@ -15,7 +19,7 @@ import pytest
 
 import pascal_poisson_fft_b200 as ppf
 from pascal_poisson_fft_b200 import workloads as W
-from _util import gpu_solve, rel_l2
+from _util import gpu_solve, oracle_solve, rel_l2
 
 pytestmark = pytest.mark.gpu
 TOL64 = 1e-12   # the FP64 tolerance of the other parity tests
@@ -36,14 +40,16 @@ def _noalloc(p):
     return P.cpu().numpy()
 
 
-def test_noalloc_matches_plan_solve_on_two_calls():
+def test_noalloc_equals_plan_solve_over_a_call_sequence():
     rng = np.random.default_rng(77)
     first = W.random_problem(rng, 64, 48, 40, (1, 1, 0), beta=1.5)
     second = W.random_problem(rng, 96, 80, 33, (0, 1, 0), beta=0.0)
-    for p in (first, second):
+    refs = {id(p): (gpu_solve(p), oracle_solve(p)) for p in (first, second)}
+    for step, p in enumerate((first, second, first, first)):
         got = _noalloc(p)
-        ref = gpu_solve(p)
-        assert rel_l2(got, ref) < TOL64
+        plan_out, oracle_out = refs[id(p)]
+        assert np.array_equal(got, plan_out), f"call {step}: differs from the plan solve"
+        assert rel_l2(got, oracle_out) < TOL64, f"call {step}: rel-L2 vs oracle"
 
 
 def test_noalloc_rejects_grids_beyond_its_array():
