@@ -12,6 +12,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libppf.so")
+CXX_OUT = os.path.join(HERE, "libppf_cxx.so")   # the C++ driver's solve calls on libppf
 BUILD = os.path.join(HERE, "_build")
 SOURCES = ["ppf_x.cu", "ppf_y.cu", "ppf_tdma.cu", "ppf_ghost.cu", "ppf_adjoint.cu", "ppf_slab.cu", "ppf_api.cu"]
 NVCC = os.environ.get("NVCC", "nvcc")
@@ -49,7 +50,25 @@ def build(verbose: bool = False, jobs: int = 4) -> str:
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
+    build_cxx_driver(verbose)
     return OUT
+
+
+def build_cxx_driver(verbose: bool = False) -> str:
+    """libppf_cxx.so: mpi_poisson::mpi_Poisson_FFT{1..5} of the C++ driver on
+    libppf (g++; found next to libppf.so through its run path).  Its
+    references to the driver's globals are resolved when the driver's
+    program (or a test harness defining them) loads it."""
+    src = os.path.join(CSRC, "ppf_cxx_driver.cpp")
+    hdrs = [os.path.join(HERE, "..", "include", h) for h in ("ppf.h", "ppf_cxx_driver.h")]
+    if _stale(CXX_OUT, [src, OUT] + hdrs):
+        cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-fopenmp",
+               "-fvisibility=hidden", "-Wall", "-o", CXX_OUT, src, f"-L{HERE}", "-l:libppf.so",
+               "-Wl,-rpath,$ORIGIN"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    return CXX_OUT
 
 
 def _wait(procs):

@@ -48,15 +48,39 @@ class _Kernels:
         _check("ppf_tdma_many_update", lib().ppf_tdma_many_update(*ptrs, n_sys, n_row, _stream_ptr(None)))
 
 
+def _host_staged(group) -> bool:
+    """Whether collectives of `group` need their CUDA tensors staged through
+    host memory (gloo moves host tensors; NCCL moves device memory)."""
+    import torch.distributed as dist
+    return dist.get_backend(group) == "gloo"
+
+
 def _torch_exchange(group):
     import torch
     import torch.distributed as dist
+    staged = _host_staged(group)
 
     def exchange(send):
+        if staged and send.is_cuda:
+            host = send.cpu()
+            recv = torch.empty_like(host)
+            dist.all_to_all_single(recv, host, group=group)
+            return recv.to(send.device)
         recv = torch.empty_like(send)
         dist.all_to_all_single(recv, send, group=group)
         return recv
     return exchange
+
+
+def all_reduce_sum(t, group=None):
+    """In-place sum over the ranks of `group` (through host memory on gloo)."""
+    import torch.distributed as dist
+    if _host_staged(group) and t.is_cuda:
+        h = t.cpu()
+        dist.all_reduce(h, group=group)
+        t.copy_(h)
+    else:
+        dist.all_reduce(t, group=group)
 
 
 def pack_reduced(a_rd, c_rd, d_rd, nranks):
@@ -171,15 +195,22 @@ def halo_exchange(P, rank, nranks, periodic, group=None):
             P[n + 1].copy_(P[1])
         return
     idx = {0: 0, 1: 1, -1: n, -2: n + 1}
-    ops = []
+    staged = _host_staged(group) and P.is_cuda
+    ops, landed = [], []
     for kind, plane, peer in halo_ops(rank, nranks, periodic):
         if kind == "send":
-            ops.append(dist.P2POp(dist.isend, P[idx[plane]].contiguous(), peer, group))
+            buf = P[idx[plane]].cpu() if staged else P[idx[plane]].contiguous()
+            ops.append(dist.P2POp(dist.isend, buf, peer, group))
         else:
-            ops.append(dist.P2POp(dist.irecv, P[idx[plane]], peer, group))
+            buf = P[idx[plane]].cpu() if staged else P[idx[plane]]
+            ops.append(dist.P2POp(dist.irecv, buf, peer, group))
+            landed.append((idx[plane], buf))
     if ops:
         for req in dist.batch_isend_irecv(ops):
             req.wait()
+    if staged:
+        for k, buf in landed:
+            P[k].copy_(buf)
 
 
 class SlabPoisson:
@@ -243,13 +274,14 @@ class SlabPoisson:
 
     # ---- the whole solve over torch.distributed ----
     def solve(self, f, P, dmx1, dmx2, dmx3_g, dx3_g, group=None):
-        import torch.distributed as dist
+        """The whole slab solve, collective over `group` (NCCL between GPUs;
+        on a gloo group the exchanges are staged through host memory)."""
         self.forward(f)
         self.coefficients(dx3_g, dmx3_g)
         tdma_many_dist(self.a, self.b, self.c, self.spec, group=group)
         self.inverse(P)
         s = self.local_sum(P).clone()
-        dist.all_reduce(s, group=group)
+        all_reduce_sum(s, group)
         s /= float(self.n[0] * self.n[1] * self.n[2])
         self.shift(P, s)
         halo_exchange(P, self.rank, self.nranks, bool(self.pbc[2]), group)

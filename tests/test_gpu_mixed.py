@@ -124,3 +124,11 @@ def test_mixed_fp32_first_iterate(shape, pbc):
     assert b.workspace_bytes() - a.workspace_bytes() == 4 * (n1 + 2) * (n2 + 2) * (n3 + 2)
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("nz", [32, 47, 97, 300, 512])
+@pytest.mark.parametrize("pbc", [(1, 1, 0), (0, 0, 0)])
+def test_mixed_z_lengths(nz, pbc):
+    rng = np.random.default_rng(nz * 5 + sum(pbc))
+    p = W.random_problem(rng, 32, 24, nz, pbc, beta=1.5)
+    assert rel_l2(gpu_solve(p, precision=PPF_MIXED, max_sweeps=3), oracle_solve(p)) < TOL_MIXED

@@ -114,3 +114,13 @@ def test_repeat_is_deterministic():
     P1, plan = gpu_solve(p, return_plan=True)
     P2 = gpu_solve(p, plan=plan)
     assert np.array_equal(P1, P2)
+
+
+@pytest.mark.parametrize("nz", [32, 47, 64, 97, 200, 256, 300, 512])
+@pytest.mark.parametrize("pbc", [(1, 1, 0), (0, 0, 0), (0, 1, 0)])
+def test_fp64_z_lengths(nz, pbc):
+    """z lengths that split into uneven row segments in the shared-memory
+    partitioned z solve (and its limits), stretched z."""
+    rng = np.random.default_rng(nz * 7 + sum(pbc))
+    p = W.random_problem(rng, 24, 20, nz, pbc, beta=2.0)
+    assert rel_l2(gpu_solve(p), oracle_solve(p)) < TOL64
