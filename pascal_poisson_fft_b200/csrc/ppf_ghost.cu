@@ -8,7 +8,7 @@
 // at one rank, :709-796, x then y then z).  Each step covers the whole face
 // including the other axes' ghost lines, so later steps read values written
 // by earlier ones; the same order is kept here, one launch per axis.
-#include "ppf_kernels.cuh"
+#include "ppf_misc_dev.cuh"
 
 #include <math.h>
 
@@ -17,36 +17,8 @@ namespace ppf {
 __global__ void k_ghost_axis(double* __restrict__ P, int dir, int neumann, int n1m, int n2m, int n3m,
                              long sy, long sz, const double* __restrict__ dmx, int faces)
 {
-    const int N1 = n1m + 2, N2 = n2m + 2, N3 = n3m + 2;
-    int nb, nm;
-    long sa, sb, sc;
-    if (dir == 0)      { nb = N2; sa = 1;  sb = sy; sc = sz; nm = n1m; }
-    else if (dir == 1) { nb = N1; sa = sy; sb = 1;  sc = sz; nm = n2m; }
-    else               { nb = N1; sa = sz; sb = 1;  sc = sy; nm = n3m; }
-    const int nc = (dir == 2) ? N2 : N3;
-    const int na = nm + 1;  // upper ghost index
-    double alo = 0, blo = 0, ahi = 0, bhi = 0;
-    if (neumann) {
-        const double d1 = dmx[1], d2 = dmx[2], dn = dmx[na], dn1 = dmx[nm];
-        const double sl = d1 + d2, su = dn + dn1;
-        alo = (sl * sl) / ((sl * sl) - d1 * d1);
-        blo = (d1 * d1) / ((sl * sl) - d1 * d1);
-        ahi = (su * su) / ((su * su) - dn * dn);
-        bhi = (dn * dn) / ((su * su) - dn * dn);
-    }
-    const long total = (long)nb * nc;
-    for (long idx = threadIdx.x + (long)blockIdx.x * blockDim.x; idx < total; idx += (long)blockDim.x * gridDim.x) {
-        const long ib = idx % nb, ic = idx / nb;
-        const long base = ib * sb + ic * sc;
-        if (neumann) {
-            if (faces & 1) P[base] = alo * P[base + sa] - blo * P[base + 2 * sa];
-            if (faces & 2) P[base + na * sa] = ahi * P[base + nm * sa] - bhi * P[base + (na - 2) * sa];
-        } else {
-            const double v0 = P[base + sa], v1 = P[base + nm * sa];
-            P[base] = v1;
-            P[base + na * sa] = v0;
-        }
-    }
+    ghost_axis(P, dir, neumann, n1m, n2m, n3m, sy, sz, dmx, faces, threadIdx.x + (long)blockIdx.x * blockDim.x,
+               (long)blockDim.x * gridDim.x);
 }
 
 cudaError_t launch_ghosts(double* P, const Geom& g, const double* dmx1, const double* dmx2, const double* dmx3,
@@ -74,41 +46,11 @@ cudaError_t launch_ghosts(double* P, const Geom& g, const double* dmx1, const do
     return cudaSuccess;
 }
 
-// After an x-inverse pass that wrote per-block partial sums: reduce them in
-// a fixed order (deterministic), keep mean(u) for the next accumulate pass,
-// and after a refinement sweep count it, record ||du||/||u|| and close the
-// gate for the remaining sweeps once it is below tol.  A sweep that was
-// skipped (gate already closed) leaves everything unchanged.
 __global__ void __launch_bounds__(512) k_sweep_gate(const double* __restrict__ partials, long nblocks, double ncell,
                                                     double* mean_prev, int* skip, int* sweeps_done, double* last_rel,
                                                     double tol, int initial)
 {
-    __shared__ double red[3][512];
-    if (*skip) return;
-    double a = 0.0, b = 0.0, c = 0.0;
-    for (long i = threadIdx.x; i < nblocks; i += blockDim.x) {
-        a += partials[3 * i + 0];
-        b += partials[3 * i + 1];
-        c += partials[3 * i + 2];
-    }
-    red[0][threadIdx.x] = a; red[1][threadIdx.x] = b; red[2][threadIdx.x] = c;
-    __syncthreads();
-    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-        if (threadIdx.x < o) {
-            red[0][threadIdx.x] += red[0][threadIdx.x + o];
-            red[1][threadIdx.x] += red[1][threadIdx.x + o];
-            red[2][threadIdx.x] += red[2][threadIdx.x + o];
-        }
-        __syncthreads();
-    }
-    if (threadIdx.x != 0) return;
-    *mean_prev = red[2][0] / ncell;
-    if (initial) return;
-    *sweeps_done += 1;
-    const double du = red[0][0], u = red[1][0];
-    const double rel = (u > 0.0) ? sqrt(du / u) : (du > 0.0 ? INFINITY : 0.0);
-    *last_rel = rel;
-    if (tol > 0.0 && rel < tol) *skip = 1;
+    sweep_gate(partials, nblocks, ncell, mean_prev, skip, sweeps_done, last_rel, tol, initial);
 }
 
 cudaError_t launch_sweep_gate(const double* partials, long nblocks, double ncell, double* mean_prev, int* skip_flag,
