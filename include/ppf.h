@@ -105,9 +105,17 @@ PPF_API int ppf_solve_adjoint(ppf_plan *plan, const double *g_d, double *df_d, c
  * (not itself capturable); every call then replays it with one graph launch
  * on `stream`.  ppf_batch_info(batch, i, info[8]): branch of problem i,
  * x tile width / run-time engine / radix order, the same for y, and the
- * number of branches (0 width = default). */
+ * number of branches (0 width = default).
+ * With PPF_BATCH_PERSISTENT the whole batch runs as one persistent kernel
+ * instead: a grid of CTAs resident on every SM takes tiles of every stage of
+ * every problem from a device work queue (stage-major across the problems),
+ * a stage starting once the problem's previous stage is complete (bounded
+ * waits); each problem gets its own work memory, the transforms use the
+ * run-time engine, and PPF_BATCH_AUTOTUNE has no effect.  The graph then
+ * holds that one launch; info reports 0 branches. */
 typedef struct ppf_batch ppf_batch;
 #define PPF_BATCH_AUTOTUNE 1
+#define PPF_BATCH_PERSISTENT 2
 PPF_API int ppf_batch_create(const ppf_desc *descs, int count, int flags, int branches, ppf_batch **batch);
 PPF_API int ppf_batch_destroy(ppf_batch *batch);
 PPF_API int ppf_batch_solve(ppf_batch *batch, const double *const *f_d, double *const *p_d,
@@ -240,6 +248,27 @@ PPF_API int ppf_slab_ghosts(ppf_plan *plan, double *p_d, const double *dmx1_d, c
 PPF_API int ppf_solve_noalloc(const ppf_desc *desc, const double *f_d, double *p_d,
                               const double *dmx1_d, const double *dmx2_d,
                               const double *dmx3_d, const double *dx3_d, void *stream);
+
+/* Ghost cells of a ghosted field P(0:n1m+1, 0:n2m+1, 0:n3m+1) on the device,
+ * outside a solve.  walls != 0: the solve's update (quadratic Neumann
+ * extrapolation along every non-periodic axis with its dmx array, then the
+ * periodic copies; cuda_neumann_BC and cuda_ghostcell_update,
+ * 01_Fortran/src/fft_3d_poisson.f90:666-852).  walls == 0: only the periodic
+ * copies, the one-rank form of the example driver's subdomain halo update
+ * (cuda_subdomain_ghostcell_update, 01_Fortran/examples/cuda_subdomain.f90:
+ * 199-220) that follows a restart load (main.f90:136-139); the dmx arrays may
+ * then be NULL.  Asynchronous on `stream`. */
+PPF_API int ppf_ghost_update(double *P_d, int n1m, int n2m, int n3m, int pbc1, int pbc2, int pbc3,
+                     const double *dmx1_d, const double *dmx2_d, const double *dmx3_d, int walls, void *stream);
+
+/* Node values of a ghosted cell field for the 3-D instant-field dump:
+ * G(i,j,k), i = 1..n1m, j = 1..n2m, k = 1..n3m, stored (n1m, n2m, n3m) x
+ * fastest, the eight-cell weighted average of calc_C2g
+ * (01_Fortran/examples/cuda_post.f90:338-353, used by
+ * cuda_Post_Fileout_InstantField_3D, :294-331).  dx1, dx2, dx3: cell widths
+ * (0:n*m+1).  Asynchronous on `stream`. */
+PPF_API int ppf_cell_to_node(const double *P_d, int n1m, int n2m, int n3m, const double *dx1_d,
+                     const double *dx2_d, const double *dx3_d, double *G_d, void *stream);
 
 /* Thread-local message describing the last error ("" if none). */
 PPF_API const char *ppf_last_error(void);

@@ -49,9 +49,11 @@ EXPORTED_SYMBOLS = (
     "ppf_stage_times", "ppf_solve_noalloc", "ppf_solve_adjoint", "ppf_batch_create", "ppf_batch_destroy",
     "ppf_batch_solve", "ppf_batch_info", "ppf_solve_host_async", "ppf_tdma_many_modified",
     "ppf_tdma_many_update", "ppf_slab_systems", "ppf_slab_forward", "ppf_slab_coefficients",
-    "ppf_slab_inverse", "ppf_slab_sum", "ppf_slab_shift", "ppf_slab_ghosts",
+    "ppf_slab_inverse", "ppf_slab_sum", "ppf_slab_shift", "ppf_slab_ghosts", "ppf_ghost_update",
+    "ppf_cell_to_node",
 )
 PPF_BATCH_AUTOTUNE = 1
+PPF_BATCH_PERSISTENT = 2
 STAGES = ("z-coefficients", "x-forward", "y-forward", "tdma-z", "y-inverse", "x-inverse",
           "refine-gate", "ghost-cells")
 
@@ -286,9 +288,11 @@ class Batch:
     """Independent problems of uneven shape solved by one graph launch.
 
     problems: sequence of dicts with keys n1m, n2m, n3m, L1, L2, pbc (3-tuple),
-    and optionally precision, max_sweeps, sweep_tol, lowk_threshold."""
+    and optionally precision, max_sweeps, sweep_tol, lowk_threshold.
+    persistent: run the batch as one persistent work-queue kernel instead of
+    per-problem kernels on concurrent branches (autotune then has no effect)."""
 
-    def __init__(self, problems, autotune=True, branches=0):
+    def __init__(self, problems, autotune=True, branches=0, persistent=False):
         descs = (_Desc * len(problems))()
         self.shapes = []
         for k, q in enumerate(problems):
@@ -299,9 +303,9 @@ class Batch:
                              float(q.get("sweep_tol", 0.0)), float(q.get("lowk_threshold", 0.0)))
             self.shapes.append((q["n3m"], q["n2m"], q["n1m"]))
         self._h = _vp()
-        _check("ppf_batch_create", lib().ppf_batch_create(descs, len(problems),
-                                                          PPF_BATCH_AUTOTUNE if autotune else 0,
-                                                          int(branches), ctypes.byref(self._h)))
+        flags = (PPF_BATCH_AUTOTUNE if autotune else 0) | (PPF_BATCH_PERSISTENT if persistent else 0)
+        _check("ppf_batch_create", lib().ppf_batch_create(descs, len(problems), flags, int(branches),
+                                                          ctypes.byref(self._h)))
 
     def __len__(self):
         return len(self.shapes)

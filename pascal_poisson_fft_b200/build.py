@@ -14,7 +14,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libppf.so")
 CXX_OUT = os.path.join(HERE, "libppf_cxx.so")   # the C++ driver's solve calls on libppf
 BUILD = os.path.join(HERE, "_build")
-SOURCES = ["ppf_x.cu", "ppf_y.cu", "ppf_tdma.cu", "ppf_ghost.cu", "ppf_adjoint.cu", "ppf_slab.cu", "ppf_api.cu"]
+SOURCES = ["ppf_x.cu", "ppf_y.cu", "ppf_tdma.cu", "ppf_ghost.cu", "ppf_adjoint.cu", "ppf_slab.cu", "ppf_batch.cu", "ppf_post.cu", "ppf_api.cu"]
 NVCC = os.environ.get("NVCC", "nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
          "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden", "--expt-relaxed-constexpr",

@@ -2,6 +2,7 @@
 #include "../../include/ppf.h"
 #include "ppf_kernels.cuh"
 #include "ppf_xy_common.cuh"
+#include "ppf_batch.cuh"
 
 #include <cuda.h>
 #include <cuda_runtime.h>
@@ -1137,6 +1138,17 @@ struct ppf_batch {
     cudaGraphExec_t exec = nullptr;
     std::vector<const void*> key;            // pointers the graph was captured with
     int dev = 0;
+    // the persistent work-queue form (PPF_BATCH_PERSISTENT): per-problem
+    // descriptors and the task queue on the device, one kernel launch
+    bool persistent = false;
+    std::vector<BProb> probs;
+    std::vector<BTask> tasks;
+    BProb* probs_d = nullptr;
+    BTask* tasks_d = nullptr;
+    int* counters_d = nullptr;                // next tile, error bits, done tiles per task
+    long total_tiles = 0;
+    size_t pers_smem = 0;
+    int pers_grid = 0;
 };
 
 namespace {
@@ -1152,7 +1164,209 @@ void free_batch(ppf_batch* b)
         if (s) cudaStreamDestroy(s);
     for (auto e : b->events)
         if (e) cudaEventDestroy(e);
+    for (void* q : { (void*)b->probs_d, (void*)b->tasks_d, (void*)b->counters_d })
+        if (q) cudaFree(q);
     delete b;
+}
+
+// ---- persistent work-queue form ----------------------------------------
+
+// widest power-of-two tile of the run-time engine for n-point lines at
+// BATCH_THREADS threads (n * W <= 8 threads) and the x tiles' line tables
+int batch_width(int n)
+{
+    int W = 1;
+    while (2 * W <= 128 && (long)n * 2 * W <= 8L * BATCH_THREADS) W *= 2;
+    return W;
+}
+
+// The stages of problem i, as solve_impl runs them, with tile counts.
+void batch_stages(const ppf_plan* p, const BProb& q, int i, std::vector<BTask>& out)
+{
+    auto add = [&](int kind, long tiles, int arg, int skip) {
+        BTask t{};
+        t.kind = kind;
+        t.prob = i;
+        t.arg = arg;
+        t.skip = skip;
+        t.tiles = (int)std::max<long>(tiles, 1);
+        t.dep = -1;
+        out.push_back(t);
+    };
+    const long ztiles = (q.z.plane + BATCH_THREADS - 1) / BATCH_THREADS;
+    auto pass = [&](int resid, int xinv_arg, int skip) {
+        add(BK_XFWD, q.x_tiles, resid, skip);
+        add(BK_YFWD, q.y_cblk * q.g.nz, 0, skip);
+        add(BK_Z, ztiles, 0, skip);
+        add(BK_YINV, q.y_cblk * q.g.nz, 0, skip);
+        add(BK_XINV, q.x_tiles, xinv_arg, skip);
+    };
+    add(BK_ZCOEF, 1, 0, 0);
+    if (p->elem == 8) {
+        pass(0, 0 | 0 | (U_P << 2), 0);
+    } else {
+        const bool mixed = p->d.precision == PPF_MIXED;
+        const bool u32 = mixed && p->d.max_sweeps > 0 && q.U;
+        pass(0, (mixed ? 2 : 0) | ((u32 ? U_WRITE : U_P) << 2), 0);
+        if (mixed) {
+            add(BK_GATE, 1, 1, 0);
+            for (int s = 0; s < p->d.max_sweeps; ++s) {
+                const bool first = u32 && s == 0;
+                pass(first ? 2 : 1, 1 | 2 | ((first ? U_ACC : U_P) << 2), 1);
+                add(BK_GATE, 1, 0, 0);
+            }
+        }
+    }
+    // ghost cells: Neumann axes first, then periodic axes (launch_ghosts' order)
+    const int per[3] = { p->g.px, p->g.py, p->g.pz };
+    const long face[3] = { (long)(p->g.ny + 2) * (p->g.nz + 2), (long)(p->g.nx + 2) * (p->g.nz + 2),
+                           (long)(p->g.nx + 2) * (p->g.ny + 2) };
+    for (int pass_ = 0; pass_ < 2; ++pass_)
+        for (int d = 0; d < 3; ++d) {
+            const bool neumann = !per[d];
+            if ((pass_ == 0) != neumann) continue;
+            add(BK_GHOST, (face[d] + BATCH_THREADS - 1) / BATCH_THREADS, d | ((neumann ? 1 : 0) << 2), 0);
+        }
+}
+
+// Per-problem work memory (every problem runs at once), descriptors and the
+// task queue in stage-major order across the problems.
+int batch_init_persistent(ppf_batch* b)
+{
+    const int count = (int)b->plans.size();
+    b->persistent = true;
+    b->probs.assign(count, BProb{});
+    std::vector<std::vector<BTask>> lists(count);
+    for (int i = 0; i < count; ++i) {
+        ppf_plan* p = b->plans[i];
+        BProb& q = b->probs[i];
+        p->sx.rt = 1;
+        p->sy.rt = 1;
+        q.wx = batch_width(p->g.nx / 2);
+        q.wy = batch_width(p->g.ny);
+        q.lgwx = ilog2i(q.wx);
+        q.lgwy = ilog2i(q.wy);
+        p->sx.w = q.wx;
+        p->sy.w = q.wy;
+        q.x_tiles = ((long)p->g.ny * p->g.nz + q.wx - 1) / q.wx;
+        q.y_cblk = (p->ycols + q.wy - 1) / q.wy;
+        const bool mixed = p->d.precision == PPF_MIXED;
+        const size_t ub = u_bytes(p);
+        void *A = nullptr, *B = nullptr, *C = nullptr, *Pt = nullptr, *Uf = nullptr;
+        if (cudaMalloc(&A, p->a_bytes) != cudaSuccess || cudaMalloc(&B, p->b_bytes) != cudaSuccess ||
+            cudaMalloc(&C, sizeof(double) * std::max<long>(p->ckpt_doubles, 1)) != cudaSuccess ||
+            (mixed && cudaMalloc(&Pt, sizeof(double) * 3 * q.x_tiles) != cudaSuccess) ||
+            (ub && cudaMalloc(&Uf, ub) != cudaSuccess)) {
+            cudaGetLastError();
+            for (void* w : { A, B, C, Pt, Uf })
+                if (w) cudaFree(w);
+            return fail(PPF_ERR_NOMEM, "cannot allocate the work memory of problem %d", i);
+        }
+        for (void* w : { A, B, C, Pt, Uf })
+            if (w) b->work.push_back(w);
+        p->A = A; p->B = B; p->ckpt = (double*)C; p->partials = (double*)Pt; p->U = (float*)Uf;
+        q.elem = (int)p->elem;
+        q.mixed = mixed ? 1 : 0;
+        q.xdct = p->xdct ? 1 : 0;
+        q.ykind = p->ykind;
+        q.cplx = p->cplx ? 1 : 0;
+        q.g = p->g;
+        ZSys& z = q.z;
+        z.mx = p->mx; z.my = p->my; z.pitch = p->b_pitch; z.plane = p->b_pitch * (long)p->my; z.nz = p->g.nz;
+        z.lamx = p->lamx; z.lamy = p->lamy; z.am = p->am; z.ap = p->ap; z.scale = p->scale;
+        z.lowk = (p->d.precision == PPF_FP64) ? 0.0 : p->d.lowk_threshold;
+        z.dzmin2 = p->scal;
+        z.dc_shift = p->scal + 4;
+        z.cyclic = p->g.pz;
+        z.ckpt = p->ckpt;
+        q.a_pitch = p->a_pitch;
+        q.a_cp = p->xdct ? p->a_pitch / 2 : p->a_pitch;
+        q.b_cp = (p->xdct && p->ydct) ? p->b_pitch / 2 : p->b_pitch;
+        q.ycols = p->ycols;
+        q.sx = p->sx;
+        q.sy = p->sy;
+        q.tw = p->tw;
+        for (int k = 0; k < 5; ++k) q.tw_off[k] = (long)p->tw_off[k];
+        q.A = A; q.B = B; q.U = (float*)Uf; q.partials = (double*)Pt;
+        q.scal = p->scal;
+        q.flags = p->flags;
+        const double hx = p->d.L1 / p->g.nx, hy = p->d.L2 / p->g.ny;
+        q.ix2 = 1.0 / (hx * hx);
+        q.iy2 = 1.0 / (hy * hy);
+        q.ncell = (double)p->g.nx * p->g.ny * p->g.nz;
+        q.sweep_tol = p->d.sweep_tol;
+        batch_stages(p, q, i, lists[i]);
+        b->info[i][0] = 0;
+        b->info[i][1] = q.wx; b->info[i][2] = 1; b->info[i][3] = 0;
+        b->info[i][4] = q.wy; b->info[i][5] = 1; b->info[i][6] = 0;
+    }
+    // stage-major queue: every problem's first stage, then every second one, ...
+    std::vector<int> at(count, 0);
+    std::vector<int> last(count, -1);
+    long first = 0;
+    for (bool more = true; more;) {
+        more = false;
+        for (int i = 0; i < count; ++i) {
+            if (at[i] >= (int)lists[i].size()) continue;
+            more = true;
+            BTask t = lists[i][at[i]++];
+            t.dep = last[i];
+            t.first = first;
+            first += t.tiles;
+            last[i] = (int)b->tasks.size();
+            b->tasks.push_back(t);
+        }
+    }
+    b->total_tiles = first;
+    const int nt = (int)b->tasks.size();
+    PPF_CK(cudaMalloc(&b->probs_d, sizeof(BProb) * count));
+    PPF_CK(cudaMalloc(&b->tasks_d, sizeof(BTask) * nt));
+    PPF_CK(cudaMalloc(&b->counters_d, sizeof(int) * (4 + (size_t)nt)));
+    PPF_CK(cudaMemcpy(b->tasks_d, b->tasks.data(), sizeof(BTask) * nt, cudaMemcpyHostToDevice));
+    b->pers_smem = batch_smem(b->probs.data(), count);
+    cudaError_t e = batch_persistent_grid(b->pers_smem, &b->pers_grid);
+    if (e != cudaSuccess) return cuda_fail(e, "persistent batch kernel occupancy");
+    b->streams.assign(1, nullptr);
+    PPF_CK(cudaStreamCreateWithFlags(&b->streams[0], cudaStreamNonBlocking));
+    return PPF_OK;
+}
+
+// One graph: the queue counters reset and the persistent kernel.
+int batch_capture_persistent(ppf_batch* b, const double* const* f, double* const* P, const double* const* m1,
+                             const double* const* m2, const double* const* m3, const double* const* x3)
+{
+    if (b->exec) {
+        cudaGraphExecDestroy(b->exec);
+        b->exec = nullptr;
+    }
+    const int count = (int)b->probs.size();
+    for (int i = 0; i < count; ++i) {
+        BProb& q = b->probs[i];
+        q.f = f[i]; q.P = P[i]; q.dmx1 = m1[i]; q.dmx2 = m2[i]; q.dmx3 = m3[i]; q.dx3 = x3[i];
+    }
+    // a launch still in flight reads the descriptors being replaced
+    PPF_CK(cudaDeviceSynchronize());
+    PPF_CK(cudaMemcpy(b->probs_d, b->probs.data(), sizeof(BProb) * count, cudaMemcpyHostToDevice));
+    cudaStream_t o = b->streams[0];
+    PPF_CK(cudaStreamBeginCapture(o, cudaStreamCaptureModeRelaxed));
+    cudaError_t e = cudaMemsetAsync(b->counters_d, 0, sizeof(int) * (4 + b->tasks.size()), o);
+    if (e == cudaSuccess)
+        e = launch_batch_persistent(b->probs_d, b->tasks_d, (int)b->tasks.size(), b->total_tiles, b->counters_d,
+                                    b->pers_smem, b->pers_grid, o);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e2 = cudaStreamEndCapture(o, &graph);
+    int rc = PPF_OK;
+    if (e != cudaSuccess) rc = cuda_fail(e, "persistent batch capture");
+    else if (e2 != cudaSuccess) rc = cuda_fail(e2, "cudaStreamEndCapture");
+    if (rc == PPF_OK) {
+        e = cudaGraphInstantiate(&b->exec, graph, 0);
+        if (e != cudaSuccess) {
+            b->exec = nullptr;
+            rc = cuda_fail(e, "cudaGraphInstantiate");
+        }
+    }
+    if (graph) cudaGraphDestroy(graph);
+    return rc;
 }
 
 struct TuneKey {
@@ -1296,6 +1510,7 @@ int batch_init(ppf_batch* b, const ppf_desc* descs, int count, int flags, int br
         rc = plan_init(p, &descs[i]);
         if (rc != PPF_OK) return rc;
     }
+    if (flags & PPF_BATCH_PERSISTENT) return batch_init_persistent(b);
     // autotune on temporary buffers sized for the largest problem
     if (flags & PPF_BATCH_AUTOTUNE) {
         size_t fa = 0, pa = 0, aa = 0, ba = 0;
@@ -1441,7 +1656,7 @@ int ppf_batch_create(const ppf_desc* descs, int count, int flags, int branches, 
     if (!batch) return fail(PPF_ERR_INVALID, "null batch pointer");
     *batch = nullptr;
     if (!descs || count < 1) return fail(PPF_ERR_INVALID, "empty batch");
-    if (flags & ~PPF_BATCH_AUTOTUNE) return fail(PPF_ERR_INVALID, "unknown batch flags 0x%x", flags);
+    if (flags & ~(PPF_BATCH_AUTOTUNE | PPF_BATCH_PERSISTENT)) return fail(PPF_ERR_INVALID, "unknown batch flags 0x%x", flags);
     ppf_batch* b = new (std::nothrow) ppf_batch();
     if (!b) return fail(PPF_ERR_NOMEM, "host allocation failed");
     int rc = batch_init(b, descs, count, flags, branches);
@@ -1478,7 +1693,8 @@ int ppf_batch_solve(ppf_batch* batch, const double* const* f_d, double* const* p
         key.insert(key.end(), { f_d[i], p_d[i], dmx1_d[i], dmx2_d[i], dmx3_d[i], dx3_d[i] });
     }
     if (!batch->exec || key != batch->key) {
-        int rc = batch_capture(batch, f_d, p_d, dmx1_d, dmx2_d, dmx3_d, dx3_d);
+        int rc = batch->persistent ? batch_capture_persistent(batch, f_d, p_d, dmx1_d, dmx2_d, dmx3_d, dx3_d)
+                                   : batch_capture(batch, f_d, p_d, dmx1_d, dmx2_d, dmx3_d, dx3_d);
         if (rc != PPF_OK) {
             batch->key.clear();
             return rc;
@@ -1489,12 +1705,39 @@ int ppf_batch_solve(ppf_batch* batch, const double* const* f_d, double* const* p
     return PPF_OK;
 }
 
+int ppf_ghost_update(double* P_d, int n1m, int n2m, int n3m, int pbc1, int pbc2, int pbc3, const double* dmx1_d,
+                     const double* dmx2_d, const double* dmx3_d, int walls, void* stream)
+{
+    g_err[0] = 0;
+    if (!P_d) return fail(PPF_ERR_INVALID, "ppf_ghost_update: null field");
+    if (n1m < 1 || n2m < 1 || n3m < 1) return fail(PPF_ERR_INVALID, "ppf_ghost_update: empty grid");
+    const int per[3] = { pbc1 ? 1 : 0, pbc2 ? 1 : 0, pbc3 ? 1 : 0 };
+    const double* dmx[3] = { dmx1_d, dmx2_d, dmx3_d };
+    if (walls)
+        for (int d = 0; d < 3; ++d)
+            if (!per[d] && !dmx[d]) return fail(PPF_ERR_INVALID, "ppf_ghost_update: wall axis %d needs its dmx", d + 1);
+    const cudaError_t e = launch_ghost_update(P_d, n1m, n2m, n3m, per, dmx, walls, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "ppf_ghost_update");
+    return PPF_OK;
+}
+
+int ppf_cell_to_node(const double* P_d, int n1m, int n2m, int n3m, const double* dx1_d, const double* dx2_d,
+                     const double* dx3_d, double* G_d, void* stream)
+{
+    g_err[0] = 0;
+    if (!P_d || !dx1_d || !dx2_d || !dx3_d || !G_d) return fail(PPF_ERR_INVALID, "ppf_cell_to_node: null array");
+    if (n1m < 1 || n2m < 1 || n3m < 1) return fail(PPF_ERR_INVALID, "ppf_cell_to_node: empty grid");
+    const cudaError_t e = launch_cell_to_node(P_d, n1m, n2m, n3m, dx1_d, dx2_d, dx3_d, G_d, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "ppf_cell_to_node");
+    return PPF_OK;
+}
+
 int ppf_batch_info(const ppf_batch* batch, int index, int* info)
 {
     if (!batch || !info) return fail(PPF_ERR_INVALID, "null argument");
     if (index < 0 || index >= (int)batch->plans.size()) return fail(PPF_ERR_INVALID, "index %d out of range", index);
     for (int k = 0; k < 8; ++k) info[k] = batch->info[index][k];
-    info[7] = (int)batch->order.size();
+    info[7] = batch->persistent ? 0 : (int)batch->order.size();
     return PPF_OK;
 }
 

@@ -120,6 +120,16 @@ cudaError_t launch_zcoef(const double* dx3, const double* dmx3, int nz, double* 
 cudaError_t launch_ghosts(double* P, const Geom& g, const double* dmx1, const double* dmx2,
                           const double* dmx3, cudaStream_t st, int zfaces = 3);
 
+// ---- field IO of the example drivers (ppf_post.cu) ----
+// ghost update of a ghosted field: walls != 0, the solve's (Neumann
+// extrapolation on non-periodic axes with dmx[d], then periodic copies);
+// walls == 0, only the periodic copies (the one-rank halo update)
+cudaError_t launch_ghost_update(double* P, int n1m, int n2m, int n3m, const int* per, const double* const* dmx,
+                                int walls, cudaStream_t st);
+// node values (n1m, n2m, n3m) of a ghosted cell field for the 3-D instant field
+cudaError_t launch_cell_to_node(const double* P, int n1m, int n2m, int n3m, const double* dx1, const double* dx2,
+                                const double* dx3, double* G, cudaStream_t st);
+
 // ---- z-slab pieces of the multi-rank solve (ppf_slab.cu) ----
 cudaError_t launch_slab_coef(double* a, double* b, double* c, double* d, long ns, int nzl, int cplx, long pitch,
                              int mx, const double* lamx, const double* lamy, const double* dx3, const double* dmx3,

@@ -78,7 +78,9 @@ __device__ __forceinline__ void coef_row(const Coef& co, int zr, typename A::T& 
         a = (CT)0; b = (CT)1; c = (CT)0;
         return;
     }
-    const double amv = __ldg(co.am + zr), apv = __ldg(co.ap + zr);
+    // plain loads: in the persistent batch kernel these tables are written
+    // earlier in the same launch, where the read-only cache is not coherent
+    const double amv = co.am[zr], apv = co.ap[zr];
     a = (CT)amv;
     c = (CT)apv;
     b = A::sub(A::sub(A::sub((CT)(-amv), (CT)apv), (CT)co.lx), (CT)co.ly);

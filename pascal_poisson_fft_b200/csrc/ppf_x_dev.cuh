@@ -16,6 +16,26 @@ namespace ppf {
 constexpr int ct_log2(int w) { return w <= 1 ? 0 : 1 + ct_log2(w / 2); }
 constexpr int MAXW = 128;  // widest tile of any shape (FP32, n = 32)
 
+// Per-line tables and reduction slots of the x tiles.  They live in
+// non-template functions so that a kernel holding several instantiations of
+// the tile bodies (the persistent batch kernel) has one copy of each, not one
+// per instantiation (static shared memory is limited to 48 KB).
+__device__ __forceinline__ long* x_line_longs()      // 3 x MAXW
+{
+    __shared__ long buf[3 * MAXW];
+    return buf;
+}
+__device__ __forceinline__ double* x_line_doubles()  // 2 x MAXW
+{
+    __shared__ double buf[2 * MAXW];
+    return buf;
+}
+__device__ __forceinline__ double* x_red_slots()     // 3 x 32
+{
+    __shared__ double buf[3 * 32];
+    return buf;
+}
+
 // n elements at base + o into L2, in bulk: the 16-byte aligned part of the
 // range (start rounded up, end rounded down), so the copy never leaves it
 template <typename U>
@@ -70,8 +90,9 @@ __device__ __forceinline__ void xfwd(const double* __restrict__ f, const ResidIn
     const int E = nc << lgW;
     // per line of the tile: offset of its first cell in the ghosted P and
     // the z coefficients of its level (no per-element division)
-    __shared__ long line_c[MAXW];
-    __shared__ double line_am[MAXW], line_ap[MAXW];
+    long* const line_c = x_line_longs();
+    double* const line_am = x_line_doubles();
+    double* const line_ap = line_am + MAXW;
     if (RESID) {
         for (int l = threadIdx.x; l < W; l += NTH) {
             const long line = line0 + l;
@@ -354,7 +375,9 @@ __device__ __forceinline__ void xinv(const void* __restrict__ in_, long in_pitch
     }
     // ghosted-output offset of each line of the tile, and (GHOST) the offsets
     // of the ghost lines its values are copied to (0: none)
-    __shared__ long line_base[MAXW], line_gy[MAXW], line_gz[MAXW];
+    long* const line_base = x_line_longs();
+    long* const line_gy = line_base + MAXW;
+    long* const line_gz = line_base + 2 * MAXW;
     bool has_yz = false;
     for (int l = threadIdx.x; l < W; l += NTH) {
         const long line = line0 + l;
@@ -446,7 +469,7 @@ __device__ __forceinline__ void xinv(const void* __restrict__ in_, long in_pitch
     }
     if (partials) {
         // deterministic per-block partial sums (reduced in a fixed order by the gate)
-        __shared__ double red[3][32];
+        double(*red)[32] = reinterpret_cast<double(*)[32]>(x_red_slots());
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) {
             acc_du += __shfl_down_sync(0xffffffffu, acc_du, off);

@@ -17,6 +17,19 @@ Fortran column-major layout.
 - Instant field (mpi_Post_FileOut_InstanField, :127-186): Tecplot ASCII
   `Output_instantfield_XY<rank tag>.plt` with the x-y plane k = (n3sub-1)/2.
 - RMS error against an exact solution (mpi_Post_error, :79-117).
+
+The GPU example driver's field IO (01_Fortran/examples/cuda_post.f90,
+main.f90), with the field in device memory (torch CUDA tensors):
+- Restart load into the device field (main.f90:136-139:
+  cuda_Post_FileIn_Continue_Post_Reassembly_IO, :224-258, then the copy to
+  the device): `cont_P.bin` holds the global interior (n1m, n2m, n3m); the
+  rank's block goes into the interior of P on the device and the ghost cells
+  get the driver's subdomain halo update, which at one rank is the periodic
+  copies along the periodic axes (ppf_ghost_update with walls = 0).
+- 3-D instant field (cuda_Post_Fileout_InstantField_3D, :294-331): Tecplot
+  ASCII `P_<rank>.PLT` of the node values, interpolated from the cells on the
+  device (ppf_cell_to_node, calc_C2g :338-353), one line
+  `(4(E11.4,1x))` per node with its face coordinates.
 """
 from __future__ import annotations
 
@@ -114,3 +127,61 @@ def rms_error(P: np.ndarray, exact: np.ndarray) -> float:
     inner = P[1:-1, 1:-1, 1:-1]
     ex = exact[1:-1, 1:-1, 1:-1] if exact.shape == P.shape else exact
     return float(np.sqrt(((inner - ex) ** 2).sum() / inner.size))
+
+
+def _fortran_e(v: float, w: int, d: int) -> str:
+    """Fortran Ew.d: 0.ddddE+ee, right-justified in w columns."""
+    return _fortran_d(v, w, d).replace("D", "E")
+
+
+def read_restart_to_device(directory: str, P, n3m_global: int, pbc, z0: int = 0, stream=None):
+    """Load this rank's block of the shared restart file `cont_P.bin` into the
+    interior of the device field P (torch CUDA float64, ghosted shape
+    (rows+2, n2m+2, n1m+2)) and fill the ghost cells as the driver's halo
+    update does at one rank: periodic copies along the periodic axes (pbc),
+    wall ghosts left as they were.  Returns P."""
+    import torch
+    from . import _check, _dptr, _stream_ptr, lib
+    host = read_restart_shared(directory, tuple(P.shape), n3m_global, z0)
+    rows, n2m, n1m = P.shape[0] - 2, P.shape[1] - 2, P.shape[2] - 2
+    staged = torch.from_numpy(np.ascontiguousarray(host[1:-1, 1:-1, 1:-1])).pin_memory()
+    P[1:-1, 1:-1, 1:-1].copy_(staged, non_blocking=True)
+    _check("ppf_ghost_update", lib().ppf_ghost_update(_dptr(P, "P"), n1m, n2m, rows, int(bool(pbc[0])),
+                                                      int(bool(pbc[1])), int(bool(pbc[2])), None, None, None, 0,
+                                                      _stream_ptr(stream)))
+    return P
+
+
+def node_field(P, dx1, dx2, dx3, stream=None):
+    """Node values (n3m, n2m, n1m) of the ghosted device field P for the 3-D
+    instant field (ppf_cell_to_node); dx* device arrays of the cell widths."""
+    import torch
+    from . import _check, _dptr, _stream_ptr, lib
+    n3m, n2m, n1m = P.shape[0] - 2, P.shape[1] - 2, P.shape[2] - 2
+    G = torch.empty((n3m, n2m, n1m), dtype=torch.float64, device=P.device)
+    _check("ppf_cell_to_node", lib().ppf_cell_to_node(_dptr(P, "P"), n1m, n2m, n3m, _dptr(dx1, "dx1", n1m + 2),
+                                                      _dptr(dx2, "dx2", n2m + 2), _dptr(dx3, "dx3", n3m + 2),
+                                                      _dptr(G, "G"), _stream_ptr(stream)))
+    return G
+
+
+def write_instant_field_3d(directory: str, P, x1, x2, x3, dx1, dx2, dx3, rank: int = 0) -> str:
+    """Tecplot ASCII 3-D instant field of the device field P:
+    `P_<rank:03d>.PLT` with the node values from the device (node_field) and
+    the face coordinates x1(i), x2(j), x3(k), i, j, k = 1..n*m, in the
+    reference's order and formats (cuda_post.f90:294-331)."""
+    G = node_field(P, dx1, dx2, dx3).cpu().numpy()
+    n3m, n2m, n1m = G.shape
+    x1, x2, x3 = (np.asarray(a, dtype=np.float64) for a in (x1, x2, x3))
+    path = os.path.join(directory, f"P_{rank:03d}.PLT")
+    with open(path, "w") as fh:
+        fh.write(' VARIABLES="X","Y","Z","P"\n')
+        fh.write(f' zone t="{1:12d}"i={n1m:12d}j={n2m:12d}k={n3m:12d}\n')
+        for k in range(1, n3m + 1):
+            zs = _fortran_e(x3[k], 11, 4) + " "
+            for j in range(1, n2m + 1):
+                ys = _fortran_e(x2[j], 11, 4) + " "
+                row = G[k - 1, j - 1]
+                fh.write("".join(_fortran_e(x1[i], 11, 4) + " " + ys + zs + _fortran_e(row[i - 1], 11, 4) + " \n"
+                                 for i in range(1, n1m + 1)))
+    return path

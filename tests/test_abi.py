@@ -53,3 +53,13 @@ def test_module_api_state_errors():
     L.ppf_cuda_poisson_fft_clean()
     assert L.ppf_cuda_poisson_fft_initial() == -5          # PPF_ERR_STATE
     assert L.ppf_cuda_poisson_fft_1d(1, 1, 1, 1, 1, 1) == -5
+
+
+def test_post_argument_validation():
+    L = ppf.lib()
+    assert L.ppf_ghost_update(None, 4, 4, 4, 1, 1, 0, None, None, None, 1, None) == -1
+    assert b"null" in L.ppf_last_error()
+    # a wall axis (z here) needs its dmx array for the Neumann extrapolation
+    assert L.ppf_ghost_update(1, 4, 4, 4, 1, 1, 0, None, None, None, 1, None) == -1
+    assert b"wall axis 3" in L.ppf_last_error()
+    assert L.ppf_cell_to_node(None, 4, 4, 4, None, None, None, None, None) == -1

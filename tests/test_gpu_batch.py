@@ -26,13 +26,14 @@ def _t(a):
     return torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float64, device=_dev())
 
 
-def _run_batch(probs, precision=PPF_FP64, autotune=True, branches=0, max_sweeps=3, batch=None, Ps=None):
+def _run_batch(probs, precision=PPF_FP64, autotune=True, branches=0, max_sweeps=3, batch=None, Ps=None,
+               persistent=False):
     import torch
     import pascal_poisson_fft_b200 as ppf
     if batch is None:
         batch = ppf.Batch([dict(n1m=p.n1m, n2m=p.n2m, n3m=p.n3m, L1=p.L1, L2=p.L2, pbc=p.pbc,
                                 precision=precision, max_sweeps=max_sweeps) for p in probs],
-                          autotune=autotune, branches=branches)
+                          autotune=autotune, branches=branches, persistent=persistent)
     fs = [_t(p.f) for p in probs]
     if Ps is None:
         Ps = [torch.zeros((p.n3m + 2, p.n2m + 2, p.n1m + 2), dtype=torch.float64, device=_dev()) for p in probs]
@@ -114,3 +115,58 @@ def test_config4_batch():
         worst = max(worst, float(torch.linalg.norm(P - R) / torch.linalg.norm(R)))
         plan.close()
     assert worst < TOL_MIXED, worst
+
+
+# ---- the persistent work-queue form (one kernel for the whole batch) ----
+
+def test_persistent_fp64_matches_oracle():
+    probs = _small_uneven(311, 10)
+    batch, Ps = _run_batch(probs, persistent=True)
+    for p, P in zip(probs, Ps):
+        assert rel_l2(P.cpu().numpy(), oracle_solve(p)) < TOL64, (p.shape, p.pbc)
+    assert all(batch.info(k)["branches"] == 0 and batch.info(k)["x_runtime"] == 1 for k in range(len(probs)))
+
+
+def test_persistent_mixed_matches_fp64_plans():
+    probs = _small_uneven(312, 12)
+    _, Ps = _run_batch(probs, precision=PPF_MIXED, persistent=True)
+    for p, P in zip(probs, Ps):
+        assert rel_l2(P.cpu().numpy(), gpu_solve(p)) < TOL_MIXED, (p.shape, p.pbc)
+
+
+def test_persistent_periodic_z_and_fp32():
+    import pascal_poisson_fft_b200 as ppf
+    rng = np.random.default_rng(313)
+    probs = [W.random_problem(rng, 32, 24, 16, (1, 1, 1)), W.random_problem(rng, 40, 48, 20, (0, 1, 1)),
+             W.random_problem(rng, 64, 32, 33, (1, 0, 0), beta=1.5)]
+    _, Ps = _run_batch(probs, persistent=True)
+    for p, P in zip(probs, Ps):
+        assert rel_l2(P.cpu().numpy(), oracle_solve(p)) < TOL64, (p.shape, p.pbc)
+    _, Ps = _run_batch(probs, precision=ppf.PPF_FP32, persistent=True)
+    for p, P in zip(probs, Ps):
+        assert rel_l2(P.cpu().numpy(), oracle_solve(p)) < 5e-5, (p.shape, p.pbc)
+
+
+def test_persistent_replay_and_new_pointers():
+    import torch
+    probs = _small_uneven(314, 6)
+    batch, Ps = _run_batch(probs, precision=PPF_MIXED, persistent=True)
+    first = [P.clone() for P in Ps]
+    _run_batch(probs, batch=batch, Ps=Ps)            # replay
+    for a, b in zip(first, Ps):
+        assert torch.equal(a, b)
+    _, Ps2 = _run_batch(probs, batch=batch)          # new output pointers
+    for a, b in zip(first, Ps2):
+        assert torch.equal(a, b)
+
+
+def test_persistent_config4_against_graph():
+    """The 96-problem workload in one persistent launch, FP64 and mixed, each
+    problem within the tolerance of the graph form's result."""
+    import torch
+    probs = W.config4(device=_dev())
+    for prec, tol in ((PPF_FP64, TOL64), (PPF_MIXED, TOL_MIXED)):
+        _, Pg = _run_batch(probs, precision=prec, max_sweeps=2)
+        _, Pp = _run_batch(probs, precision=prec, max_sweeps=2, persistent=True)
+        worst = max(float(torch.linalg.norm(a - b) / torch.linalg.norm(b)) for a, b in zip(Pp, Pg))
+        assert worst < tol, (prec, worst)
