@@ -118,6 +118,10 @@ def lib() -> ctypes.CDLL:
     L.ppf_batch_destroy.argtypes = [_vp]
     L.ppf_batch_solve.argtypes = [_vp] + [ctypes.POINTER(_vp)] * 6 + [_vp]
     L.ppf_batch_info.argtypes = [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+    L.ppf_ghost_update.argtypes = [_vp] + [ctypes.c_int] * 6 + [_vp] * 3 + [ctypes.c_int, _vp]
+    L.ppf_cell_to_node.argtypes = [_vp] + [ctypes.c_int] * 3 + [_vp] * 5
+    for name in ("ppf_last_error", "ppf_version", "ppf_cuda_poisson_fft_initial", "ppf_cuda_poisson_fft_clean"):
+        getattr(L, name).argtypes = []
     for name in EXPORTED_SYMBOLS:
         if name not in ("ppf_last_error", "ppf_version"):
             getattr(L, name).restype = ctypes.c_int

@@ -20,14 +20,19 @@ __global__ void __launch_bounds__(256) k_cell_to_node(const double* __restrict__
         const int i = (int)(q % n1m) + 1, j = (int)((q / n1m) % n2m) + 1, k = (int)(q / ((long)n1m * n2m)) + 1;
         const int im = i - 1, jm = j - 1, km = k - 1;
         auto X = [&](int a, int b, int c) { return P[a + b * sy + c * sz]; };
-        const double wz = dx3[k] + dx3[km], wx = dx1[i] + dx1[im];
-        double X1 = (X(im, jm, k) * dx3[km] + X(im, jm, km) * dx3[k]) / wz;
-        double X2 = (X(i, jm, k) * dx3[km] + X(i, jm, km) * dx3[k]) / wz;
-        const double Xy1 = (X2 * dx1[im] + X1 * dx1[i]) / wx;
-        X1 = (X(im, j, k) * dx3[km] + X(im, j, km) * dx3[k]) / wz;
-        X2 = (X(i, j, k) * dx3[km] + X(i, j, km) * dx3[k]) / wz;
-        const double Xy2 = (X2 * dx1[im] + X1 * dx1[i]) / wx;
-        G[q] = (Xy2 * dx2[jm] + Xy1 * dx2[j]) / (dx2[j] + dx2[jm]);
+        // (p * wp + q * wq) / w with each product and sum rounded on its own
+        // (no fused multiply-add), as the CPU evaluates it
+        auto lerp = [](double p, double wp, double q, double wq, double w) {
+            return __dadd_rn(__dmul_rn(p, wp), __dmul_rn(q, wq)) / w;
+        };
+        const double wz = __dadd_rn(dx3[k], dx3[km]), wx = __dadd_rn(dx1[i], dx1[im]);
+        double X1 = lerp(X(im, jm, k), dx3[km], X(im, jm, km), dx3[k], wz);
+        double X2 = lerp(X(i, jm, k), dx3[km], X(i, jm, km), dx3[k], wz);
+        const double Xy1 = lerp(X2, dx1[im], X1, dx1[i], wx);
+        X1 = lerp(X(im, j, k), dx3[km], X(im, j, km), dx3[k], wz);
+        X2 = lerp(X(i, j, k), dx3[km], X(i, j, km), dx3[k], wz);
+        const double Xy2 = lerp(X2, dx1[im], X1, dx1[i], wx);
+        G[q] = lerp(Xy2, dx2[jm], Xy1, dx2[j], __dadd_rn(dx2[j], dx2[jm]));
     }
 }
 

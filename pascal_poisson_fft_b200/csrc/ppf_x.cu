@@ -159,8 +159,22 @@ __global__ void __launch_bounds__(SH::NT, (SH::N == 384 || SH::N <= 128) ? 2 : 0
         // one line
         auto zout = [&](int n, int l, cx<T> zv) {
             if (line0 + l >= nlines) return;
-            const double x0 = (double)zv.x, x1 = (double)zv.y;
             const long o = line_base[l] + 2 * n;
+            if constexpr (UK == U_WRITE && !ACC && sizeof(T) == 4) {
+                // the FP32 first iterate: the values go out as they are, and
+                // only their sum is kept (the initial gate after this pass
+                // needs the mean, not the norms)
+                U[o] = zv.x;
+                U[o + 1] = zv.y;
+                if (GHOST && yz) {
+                    const long gy = line_gy[l], gz = line_gz[l];
+                    if (gy) { U[o + gy] = zv.x; U[o + 1 + gy] = zv.y; }
+                    if (gz) { U[o + gz] = zv.x; U[o + 1 + gz] = zv.y; }
+                }
+                if (partials) acc_s += (double)zv.x + (double)zv.y;
+                return;
+            }
+            const double x0 = (double)zv.x, x1 = (double)zv.y;
             double u0 = x0, u1 = x1;
             if (ACC) {
                 u0 = (src(o) - mprev) + x0;
@@ -174,8 +188,11 @@ __global__ void __launch_bounds__(SH::NT, (SH::N == 384 || SH::N <= 128) ? 2 : 0
                 if (gz) { put(o + gz, u0); put(o + 1 + gz, u1); }
             }
             if (partials) {
-                acc_du += x0 * x0 + x1 * x1;
-                acc_u += u0 * u0 + u1 * u1;
+                // the norms feed the gate after a refinement sweep only
+                if (ACC) {
+                    acc_du += x0 * x0 + x1 * x1;
+                    acc_u += u0 * u0 + u1 * u1;
+                }
                 acc_s += u0 + u1;
             }
         };

@@ -429,8 +429,11 @@ __device__ __forceinline__ void xinv(const void* __restrict__ in_, long in_pitch
                 if (gz) { put(o + gz, u0); put(o + 1 + gz, u1); }
             }
             if (partials) {
-                acc_du += x0 * x0 + x1 * x1;
-                acc_u += u0 * u0 + u1 * u1;
+                // the norms feed the gate after a refinement sweep only
+                if (ACC) {
+                    acc_du += x0 * x0 + x1 * x1;
+                    acc_u += u0 * u0 + u1 * u1;
+                }
                 acc_s += u0 + u1;
             }
         }
@@ -457,8 +460,10 @@ __device__ __forceinline__ void xinv(const void* __restrict__ in_, long in_pitch
                 if (gz) put(o + gz, un);
             }
             if (partials) {
-                acc_du += x * x;
-                acc_u += un * un;
+                if (ACC) {
+                    acc_du += x * x;
+                    acc_u += un * un;
+                }
                 acc_s += un;
             }
         }

@@ -25,6 +25,36 @@ def test_library_exports_every_header_symbol():
         assert hasattr(L, name), name
 
 
+def header_prototypes():
+    """name -> list of parameter declarations, from include/ppf.h"""
+    txt = open(os.path.join(ROOT, "include", "ppf.h")).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    out = {}
+    for m in re.finditer(r"PPF_API\s+(?:const\s+)?\w+\s*\*?\s*(ppf_\w+)\s*\(([^)]*)\)", txt):
+        params = " ".join(m.group(2).split())
+        out[m.group(1)] = [] if params in ("", "void") else [p.strip() for p in params.split(",")]
+    return out
+
+
+def test_every_binding_declares_its_argument_types():
+    """Without argtypes ctypes passes a Python int as a 32-bit C int, which
+    truncates device pointers and stream handles: every exported function
+    has them, one per declared parameter, pointer parameters as pointers."""
+    import ctypes
+    L = ppf.lib()
+    for name, params in header_prototypes().items():
+        at = getattr(L, name).argtypes
+        assert at is not None, name
+        assert len(at) == len(params), (name, len(at), params)
+        for decl, t in zip(params, at):
+            if "*" in decl:
+                assert t is ctypes.c_void_p or issubclass(t, ctypes._Pointer), (name, decl, t)
+            elif decl.split()[0] == "int":
+                assert t is ctypes.c_int, (name, decl, t)
+            elif decl.split()[0] == "double":
+                assert t is ctypes.c_double, (name, decl, t)
+
+
 def test_version_string():
     assert b"sm_100a" in ppf.lib().ppf_version()
 

@@ -43,7 +43,8 @@ def test_cell_to_node_matches_the_reference_formula():
     dx = [rng.uniform(0.5, 1.5, n + 2) for n in (n1, n2, n3)]
     dx[2][0] = 0.0   # a wall below the first cell, as the driver's metric has
     G = io.node_field(_t(P), *[_t(d) for d in dx]).cpu().numpy()
-    np.testing.assert_allclose(G, c2g_reference(P, *dx), rtol=1e-14, atol=0)
+    # the same products, sums and quotients in the same order: bit-exact
+    np.testing.assert_array_equal(G, c2g_reference(P, *dx))
 
 
 def test_instant_field_3d_file(tmp_path):
@@ -101,6 +102,7 @@ def test_ghost_update_matches_the_oracle(pbc):
     ref = P.copy()
     O.fill_ghosts(ref, pbc, *dmx)
     Pd = _t(P)
-    rc = ppf.lib().ppf_ghost_update(Pd.data_ptr(), n1, n2, n3, *pbc, *[_t(d).data_ptr() for d in dmx], 1, None)
+    dmx_d = [_t(d) for d in dmx]   # held: a freed block would be handed to the next array
+    rc = ppf.lib().ppf_ghost_update(Pd.data_ptr(), n1, n2, n3, *pbc, *[d.data_ptr() for d in dmx_d], 1, None)
     assert rc == 0, ppf.lib().ppf_last_error()
     np.testing.assert_allclose(Pd.cpu().numpy(), ref, rtol=1e-14, atol=1e-15)
