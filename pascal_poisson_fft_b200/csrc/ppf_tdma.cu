@@ -34,12 +34,49 @@
 #include "ppf_kernels.cuh"
 #include "ppf_tdma_dev.cuh"
 #include "ppf_misc_dev.cuh"
+#include "ppf_tma.cuh"
 
 #include <math.h>
+#include <mutex>
 
 namespace ppf {
 
 using namespace zdev;
+
+namespace {
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// dependency on libcuda)
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiled encode_tiled()
+{
+    static EncodeTiled fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiled>(p);
+    });
+    return fn;
+}
+}  // namespace
+
+bool tma_map_2d_f32(CUtensorMap* map, void* base, unsigned long long inner, unsigned long long rows,
+                    unsigned long long row_bytes, unsigned box_inner, unsigned box_rows)
+{
+    const EncodeTiled enc = encode_tiled();
+    if (!enc) return false;
+    const cuuint64_t dims[2] = { inner, rows };
+    const cuuint64_t strides[1] = { row_bytes };
+    const cuuint32_t box[2] = { box_inner, box_rows };
+    const cuuint32_t estr[2] = { 1, 1 };
+    return enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
 
 // MODE 0: every system, arithmetic A.  MODE 1: only systems above the
 // low-wavenumber threshold (FP32 path).  MODE 2: only systems below it.
@@ -95,6 +132,72 @@ int* tdma_z_lowk_list(double* ckpt, int nz, long plane, int cyclic)
 }
 
 namespace {
+// One chunk of C rows from z0 of the FP32 bulk sweep: the forward
+// elimination from the state (cp, dr, di) ending the previous chunk, c' and
+// d' of every row kept in cs, vr, vi (vr, vi enter as the right-hand
+// sides).  zlev[k] = (am, ap, -am - ap) of level k; rows from nz on are
+// skipped.
+template <bool CPLX, int C>
+__device__ __forceinline__ void fast_chunk_elim(const float4* zlev, float lamf, int nz, int z0, float* vr, float* vi,
+                                                float* cs, float& cp, float& dr, float& di)
+{
+    if (z0 == 0) {
+        const float4 l0 = zlev[0];
+        fwd_row<Fast, CPLX>(true, l0.x, l0.z - lamf, l0.y, vr[0], vi[0], cp, dr, di);
+        cs[0] = cp; vr[0] = dr; vi[0] = di;
+#pragma unroll
+        for (int q = 1; q < C; ++q) {
+            if (q < nz) {
+                const float4 lv = zlev[q];
+                fwd_row<Fast, CPLX>(false, lv.x, lv.z - lamf, lv.y, vr[q], vi[q], cp, dr, di);
+            }
+            cs[q] = cp; vr[q] = dr; vi[q] = di;
+        }
+    } else if (z0 + C <= nz) {
+#pragma unroll
+        for (int q = 0; q < C; ++q) {
+            const float4 lv = zlev[z0 + q];
+            fwd_row<Fast, CPLX>(false, lv.x, lv.z - lamf, lv.y, vr[q], vi[q], cp, dr, di);
+            cs[q] = cp; vr[q] = dr; vi[q] = di;
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < C; ++q) {
+            if (z0 + q < nz) {
+                const float4 lv = zlev[z0 + q];
+                fwd_row<Fast, CPLX>(false, lv.x, lv.z - lamf, lv.y, vr[q], vi[q], cp, dr, di);
+            }
+            cs[q] = cp; vr[q] = dr; vi[q] = di;
+        }
+    }
+}
+
+// The back substitution of that chunk, top row first, from x of the row
+// above (xr, xi); each solution row is scaled and stored at col + row * pl,
+// and added to fsum (the non-finite check).
+template <bool CPLX, int C, typename E>
+__device__ __forceinline__ void fast_chunk_subst(E* col, unsigned pl, int nz, int z0, const float* vr,
+                                                 const float* vi, const float* cs, float sc, float& xr, float& xi,
+                                                 float& fsum)
+{
+    auto put = [&](int q) {
+        xr = vr[q] - cs[q] * xr;
+        if (CPLX) xi = vi[q] - cs[q] * xi;
+        fsum += xr + xi;
+        E* o = col + (size_t)(unsigned)(z0 + q) * pl;
+        if constexpr (CPLX) *o = mk<float>(xr * sc, xi * sc);
+        else *o = xr * sc;
+    };
+    if (z0 + C <= nz) {
+#pragma unroll
+        for (int q = C - 1; q >= 0; --q) put(q);
+    } else {
+#pragma unroll
+        for (int q = C - 1; q >= 0; --q)
+            if (z0 + q < nz) put(q);
+    }
+}
+
 // FP32 bulk of the mixed-precision z solve (systems with lam dz_min^2 >=
 // lowk, non-periodic z).  The same Thomas sweep as thomas_poisson<Fast>,
 // with the level coefficients (am, ap, -am-ap) staged once per CTA in shared
@@ -147,38 +250,6 @@ __global__ void __launch_bounds__(TPB, CPLX ? 7 : 6) k_thomas_fast(void* __restr
             }
         }
     };
-    // rows [q0, q1) of a chunk from state (cp, dr, di); keep: c', d' per row
-    auto elim = [&](int z0, float* vr, float* vi, float* cs, float& cp, float& dr, float& di) {
-        if (z0 == 0) {
-            const float4 l0 = zlev[0];
-            fwd_row<Fast, CPLX>(true, l0.x, l0.z - lamf, l0.y, vr[0], vi[0], cp, dr, di);
-            cs[0] = cp; vr[0] = dr; vi[0] = di;
-#pragma unroll
-            for (int q = 1; q < C; ++q) {
-                if (q < nz) {
-                    const float4 lv = zlev[q];
-                    fwd_row<Fast, CPLX>(false, lv.x, lv.z - lamf, lv.y, vr[q], vi[q], cp, dr, di);
-                }
-                cs[q] = cp; vr[q] = dr; vi[q] = di;
-            }
-        } else if (z0 + C <= nz) {
-#pragma unroll
-            for (int q = 0; q < C; ++q) {
-                const float4 lv = zlev[z0 + q];
-                fwd_row<Fast, CPLX>(false, lv.x, lv.z - lamf, lv.y, vr[q], vi[q], cp, dr, di);
-                cs[q] = cp; vr[q] = dr; vi[q] = di;
-            }
-        } else {
-#pragma unroll
-            for (int q = 0; q < C; ++q) {
-                if (z0 + q < nz) {
-                    const float4 lv = zlev[z0 + q];
-                    fwd_row<Fast, CPLX>(false, lv.x, lv.z - lamf, lv.y, vr[q], vi[q], cp, dr, di);
-                }
-                cs[q] = cp; vr[q] = dr; vi[q] = di;
-            }
-        }
-    };
     load(0);
     float cp = 0.f, dr = 0.f, di = 0.f;
     for (int ch = 0; ch < nch; ++ch) {
@@ -186,7 +257,7 @@ __global__ void __launch_bounds__(TPB, CPLX ? 7 : 6) k_thomas_fast(void* __restr
 #pragma unroll
         for (int q = 0; q < C; ++q) { vr[q] = nr[q]; vi[q] = ni[q]; }
         if (ch + 1 < nch) load((ch + 1) * C);
-        elim(ch * C, vr, vi, cs, cp, dr, di);
+        fast_chunk_elim<CPLX, C>(zlev, lamf, nz, ch * C, vr, vi, cs, cp, dr, di);
         float* c3 = ckw + (size_t)(unsigned)(3 * ch) * pl;
         c3[0] = cp;
         c3[pl] = dr;
@@ -217,35 +288,383 @@ __global__ void __launch_bounds__(TPB, CPLX ? 7 : 6) k_thomas_fast(void* __restr
                 kc = 0.f; kr = 0.f; ki = 0.f;
             }
         }
-        const int z0 = ch * C;
-        elim(z0, vr, vi, cs, pcp, pdr, pdi);
-        if (z0 + C <= nz) {
-#pragma unroll
-            for (int q = C - 1; q >= 0; --q) {
-                xr = vr[q] - cs[q] * xr;
-                if (CPLX) xi = vi[q] - cs[q] * xi;
-                fsum += xr + xi;
-                E* o = row(z0 + q);
-                if constexpr (CPLX) *o = mk<float>(xr * sc, xi * sc);
-                else *o = xr * sc;
-            }
-        } else {
-#pragma unroll
-            for (int q = C - 1; q >= 0; --q) {
-                if (z0 + q < nz) {
-                    xr = vr[q] - cs[q] * xr;
-                    if (CPLX) xi = vi[q] - cs[q] * xi;
-                    fsum += xr + xi;
-                    E* o = row(z0 + q);
-                    if constexpr (CPLX) *o = mk<float>(xr * sc, xi * sc);
-                    else *o = xr * sc;
-                }
-            }
-        }
+        fast_chunk_elim<CPLX, C>(zlev, lamf, nz, ch * C, vr, vi, cs, pcp, pdr, pdi);
+        fast_chunk_subst<CPLX, C>(col, pl, nz, ch * C, vr, vi, cs, sc, xr, xi, fsum);
     }
     if (!isfinite(fsum) && err) atomicOr(err, 1);
 }
 
+// The FP32 bulk sweep with the field streamed through shared memory.  One
+// persistent CTA per SM walks blocks of W consecutive FP32 values of a z
+// row; each value's column is one tridiagonal system (the real and the
+// imaginary part of a complex system are two columns with the same
+// coefficients).  Each column is solved by a twisted factorisation with two
+// threads: one eliminates the lower half top-down (Thomas: r = 1/(b - a c'),
+// c' = r c, d' = r (d - a d')), the other the upper half bottom-up
+// (r = 1/(b - c a''), a'' = r a, d'' = r (d - c d'')), the two halves meet
+// in a 2 x 2 solve for the middle rows, and each thread then substitutes
+// outwards through its half (x = d' - c' x_above, x = d'' - a'' x_below).
+// Rows arrive as TMA boxes (R rows x W values, one box of each half per
+// step) through a ring of `stages` buffers, several steps ahead; the
+// elimination keeps chunk checkpoints in shared memory and the
+// substitution loads its chunks again and recomputes their c', d' (a'', d'')
+// from the checkpoints.  With one block per SM in flight, the columns
+// between a first read and their re-read (SMs x W x nz values: 78 MB at 512
+// levels) fit in the L2 cache, which serves the re-read (first reads with
+// the evict_last priority, re-reads with evict_first), so each value
+// crosses the HBM interface once each way.  The FFT normalisation is folded
+// into the staged coefficients (A/s solves for s x) and the reciprocals are
+// the approximate ones: the FP64 refinement absorbs this path's rounding.
+__device__ __forceinline__ float rcp_approx(float x)
+{
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+struct ZStream {
+    static constexpr int W = 224;        // columns per block and box row
+    static constexpr int NC = 2 * W;     // consumer threads: lower half, upper half of each column
+    static constexpr int NT = NC + 32;   // + the producer warp
+    static constexpr int R = 16;         // rows per box and checkpoint chunk
+    static constexpr int MAX_STAGES = 8;
+    static constexpr unsigned BOX = (unsigned)(R * W * sizeof(float));
+    static constexpr unsigned STAGE = 2 * BOX;   // one box of each half
+    static __host__ __device__ int nch(int nz) { return (nz + R - 1) / R; }
+    static __host__ __device__ size_t ck_bytes(int nz) { return (size_t)nch(nz) * 2 * W * sizeof(float); }
+    // + the middle exchange, 4 values per column, for two blocks
+    static size_t smem(int nz, int stages)
+    {
+        return 128 + (size_t)stages * STAGE + ck_bytes(nz) + sizeof(float4) * (size_t)nz + 8 * W * sizeof(float);
+    }
+};
+// Bound of a wait for one step's boxes: polls that each sleep up to
+// ZS_POLL_NS while the boxes are in flight (about 2 s in all): far above any
+// load time, so it only ends a kernel whose copies never complete, with err
+// bit 2 set.
+constexpr unsigned ZS_POLL_NS = 20000;
+constexpr long ZS_WAIT_LIMIT = 100000;
+
+// The level coefficients are staged over the FFT normalisation n:
+// zlev[k] = (am_k, ap_k, -am_k - ap_k) / n, and lam / n with them, so the
+// sweeps solve (A / n) y = rhs for y = n x.
+
+// Rows z0 .. z0+R-1 of the lower half, eliminated top-down from the state
+// (e, d) = (c', d') of the row below z0 (r = 1/(b - a e), c' = r c,
+// d' = r (d - a d')); the sweep starts from (0, 0), for which the general
+// step is the first row's.  KEEP: c', d' of every row into g, v (v enters
+// as the right-hand sides).
+template <bool KEEP>
+__device__ __forceinline__ void zs_down(const float4* zlev, float lam, int z0, float* v, float* g, float& e, float& d)
+{
+#pragma unroll
+    for (int q = 0; q < ZStream::R; ++q) {
+        const float4 zl = zlev[z0 + q];
+        const float r = rcp_approx((zl.z - lam) - zl.x * e);
+        d = r * (v[q] - zl.x * d);
+        e = r * zl.y;
+        if (KEEP) { g[q] = e; v[q] = d; }
+    }
+}
+// Rows z0+R-1 .. z0 of the upper half, eliminated bottom-up from the state
+// (e, d) = (a'', d'') of the row above (r = 1/(b - c e), a'' = r a,
+// d'' = r (d - c d'')); TOP: the chunk holds the top row nz-1, rows from nz
+// on are skipped.
+template <bool TOP, bool KEEP>
+__device__ __forceinline__ void zs_up(const float4* zlev, float lam, int z0, int nz, float* v, float* g, float& e,
+                                      float& d)
+{
+#pragma unroll
+    for (int q = ZStream::R - 1; q >= 0; --q) {
+        if (!TOP || z0 + q < nz) {
+            const float4 zl = zlev[z0 + q];
+            const float r = rcp_approx((zl.z - lam) - zl.y * e);
+            d = r * (v[q] - zl.y * d);
+            e = r * zl.x;
+        }
+        if (KEEP) { g[q] = e; v[q] = d; }
+    }
+}
+
+// OR of `pred` over the `n` threads of named barrier `id` (a warp-multiple
+// subset of the CTA), which all wait there
+__device__ __forceinline__ bool bar_or(int id, int n, bool pred)
+{
+    unsigned r;
+    asm volatile("{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n bar.red.or.pred q, %2, %3, p;\n"
+                 " selp.u32 %0, 1, 0, q;\n}\n"
+                 : "=r"(r)
+                 : "r"((unsigned)pred), "r"(id), "r"(n)
+                 : "memory");
+    return r != 0;
+}
+
+// CPLX: complex systems, value u of a row is part (u & 1) of system u >> 1.
+// The ring is a producer/consumer pipeline: full[b] completes when the
+// boxes of the step in buffer b have landed, empty[b] when every consumer
+// warp has finished reading them, and a producer warp refills each buffer
+// as soon as its empty phase completes, so the loads run ahead of the
+// slowest warp by the ring's depth.  The consumers meet once per block (the
+// middle exchange, double-buffered by block) at a named barrier, which
+// also carries the vote on a wait that gave up.
+template <bool CPLX>
+__global__ void __launch_bounds__(ZStream::NT, 1)
+    k_thomas_stream(const __grid_constant__ CUtensorMap tmap, void* __restrict__ data_, ZSys z, int stages,
+                    const int* __restrict__ skip, int* __restrict__ err)
+{
+    if (skip && *skip) return;
+    using S = ZStream;
+    constexpr int W = S::W, R = S::R, SH = CPLX ? 1 : 0, NC = S::NC;
+    extern __shared__ __align__(128) unsigned char zs_raw[];
+    __shared__ __align__(8) uint64_t full[S::MAX_STAGES];
+    __shared__ __align__(8) uint64_t empty[S::MAX_STAGES];
+    __shared__ int abort_flag;
+    unsigned char* const base = reinterpret_cast<unsigned char*>(((uintptr_t)zs_raw + 127) & ~(uintptr_t)127);
+    float* const ring = reinterpret_cast<float*>(base);
+    const int nz = z.nz, nch = S::nch(nz);
+    const int hl = nch / 2, hu = nch - hl;   // chunks of the lower and the upper half (hu >= 1)
+    float* const ck = reinterpret_cast<float*>(base + (size_t)stages * S::STAGE);
+    float4* const zlev = reinterpret_cast<float4*>(base + (size_t)stages * S::STAGE + S::ck_bytes(nz));
+    float* const xch = reinterpret_cast<float*>(zlev + nz);
+    const int tid = threadIdx.x, lane = tid & 31;
+    const long nval = z.plane << SH;     // values per z row
+    const long nblk = (nval + W - 1) / W;
+    const long mine = (long)blockIdx.x < nblk ? (nblk - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+    const long total = mine * 2 * hu;    // steps of this CTA, in order
+    volatile int* const abort_v = &abort_flag;
+    if (tid == 0) {
+        for (int q = 0; q < stages; ++q) {
+            mbar_init(&full[q], 1);
+            mbar_init(&empty[q], NC / 32);
+        }
+        mbar_init_fence();
+        abort_flag = 0;
+    }
+    const double isc = 1.0 / z.scale;
+    for (int k = tid; k < nz; k += S::NT) {
+        const double am = z.am[k], ap = z.ap[k];
+        zlev[k] = make_float4((float)(am * isc), (float)(ap * isc), (float)((-am - ap) * isc), 0.f);
+    }
+    __syncthreads();
+
+    if (tid >= NC) {
+        // ---- producer warp (one thread): step p of block iteration p_it is
+        // elimination step j = p_pos (< hu) or substitution step j = p_pos - hu
+        if (tid != NC) return;
+        const uint64_t pol_keep = l2_policy_evict_last(), pol_drop = l2_policy_evict_first();
+        long issued = 0, p_it = 0, p_round = 0;
+        int p_pos = 0, p_buf = 0;
+        bool ok = true;
+        while (issued < total) {
+            if (p_round > 0) {   // the buffer's previous step has been read by every consumer warp
+                ok = false;
+                for (long q = 0; q < ZS_WAIT_LIMIT && !ok; ++q) {
+                    ok = mbar_try_wait_sleep(&empty[p_buf], (unsigned)((p_round - 1) & 1), ZS_POLL_NS);
+                    if (!ok && *abort_v) break;
+                }
+                if (!ok) break;
+            }
+            const bool elim = p_pos < hu;
+            const int j = elim ? p_pos : p_pos - hu;
+            const int cl = elim ? j : hl - 1 - j;            // lower chunk (if j < hl)
+            const int cu = elim ? nch - 1 - j : hl + j;      // upper chunk
+            const bool has_l = j < hl;
+            const long blk = blockIdx.x + p_it * gridDim.x;
+            float* dst = ring + (size_t)p_buf * 2 * R * W;
+            const uint64_t pol = elim ? pol_keep : pol_drop;
+            fence_proxy_async_smem();   // the consumers' reads of the buffer come before its refill
+            mbar_arrive_expect_tx(&full[p_buf], has_l ? S::STAGE : S::BOX);
+            if (has_l) tma_load_2d(dst, &tmap, (int)(blk * W), cl * R, &full[p_buf], pol);
+            tma_load_2d(dst + R * W, &tmap, (int)(blk * W), cu * R, &full[p_buf], pol);
+            ++issued;
+            if (++p_pos == 2 * hu) { p_pos = 0; ++p_it; }
+            if (++p_buf == stages) { p_buf = 0; ++p_round; }
+        }
+        if (!ok) {
+            *abort_v = 1;
+            if (err) atomicOr(err, 2);
+        }
+        // the last load into every buffer has landed before the CTA's shared
+        // memory can be released
+        for (int b = 0; b < stages; ++b) {
+            const long nb = issued > b ? (issued - 1 - b) / stages + 1 : 0;   // loads into buffer b
+            if (nb > 0) mbar_wait_sleep_bounded(&full[b], (unsigned)((nb - 1) & 1), ZS_POLL_NS, ZS_WAIT_LIMIT);
+        }
+        return;
+    }
+
+    // ---- consumers
+    const bool upper = tid >= W;
+    const int col_i = upper ? tid - W : tid;
+    const double dzmin2 = __ldg(z.dzmin2);
+    int c_buf = 0;
+    unsigned c_par = 0;
+    // the boxes of the next step have landed; false: a wait gave up, here
+    // or elsewhere (the abort flag)
+    auto ready = [&]() -> bool {
+        for (long q = 0; q < ZS_WAIT_LIMIT; ++q) {
+            if (mbar_try_wait_sleep(&full[c_buf], c_par, ZS_POLL_NS)) return true;
+            if (*abort_v) return false;
+        }
+        *abort_v = 1;
+        if (err) atomicOr(err, 2);
+        return false;
+    };
+    // this warp is done with the boxes of the step
+    auto release = [&]() {
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[c_buf]);
+        if (++c_buf == stages) { c_buf = 0; c_par ^= 1u; }
+    };
+    const unsigned pl = (unsigned)nval;
+    float fsum = 0.f;
+    bool failed = false;
+    for (long i = 0; i < mine; ++i) {
+        const long u = (blockIdx.x + i * gridDim.x) * W + col_i;
+        const long sys = u >> SH;
+        const int kx = (int)(sys % z.pitch), ky = (int)(sys / z.pitch);
+        bool act = u < nval && kx < z.mx && ky < z.my;
+        float lam = 0.f;
+        if (act) {
+            const double l = z.lamx[kx] + z.lamy[ky];
+            act = !(l * dzmin2 < z.lowk);   // else solved in FP64 (the pinned zero mode among them)
+            lam = (float)(l * isc);
+        }
+        // ---- elimination: the lower half top-down over chunks 0 .. hl-1,
+        // the upper half bottom-up over chunks nch-1 .. hl
+        float e = 0.f, d = 0.f;   // lower: c', d'; upper: a'', d''
+        for (int j = 0; j < hu && !failed; ++j) {
+            if (!ready()) { failed = true; break; }
+            if (act && (upper || j < hl)) {
+                const float* t = ring + (size_t)c_buf * 2 * R * W + (upper ? R * W : 0) + col_i;
+                float v[R];
+#pragma unroll
+                for (int q = 0; q < R; ++q) v[q] = t[q * W];
+                float* k2;
+                if (!upper) {
+                    zs_down<false>(zlev, lam, j * R, v, nullptr, e, d);   // lower chunks are full
+                    k2 = ck + (size_t)j * 2 * W + col_i;
+                } else {
+                    const int c = nch - 1 - j;
+                    if (j == 0) zs_up<true, false>(zlev, lam, c * R, nz, v, nullptr, e, d);
+                    else zs_up<false, false>(zlev, lam, c * R, nz, v, nullptr, e, d);
+                    k2 = ck + (size_t)c * 2 * W + col_i;
+                }
+                k2[0] = e;
+                k2[W] = d;
+            }
+            release();
+        }
+        // ---- the middle rows m-1 (lower) and m (upper): x_{m-1} + c' x_m = d',
+        // a'' x_{m-1} + x_m = d''
+        float* const xb = xch + (i & 1) * 4 * W;
+        if (upper) { xb[2 * W + col_i] = e; xb[3 * W + col_i] = d; }
+        else { xb[col_i] = e; xb[W + col_i] = d; }
+        if (bar_or(1, NC, failed)) { failed = true; break; }
+        float x = 0.f;   // lower: x of the row above; upper: x of the row below
+        {
+            const float cl = hl ? xb[col_i] : 0.f, dl = hl ? xb[W + col_i] : 0.f;
+            const float au = xb[2 * W + col_i], du = xb[3 * W + col_i];
+            const float xm = (du - au * dl) / (1.f - au * cl);
+            x = upper ? dl - cl * xm : xm;
+        }
+        // ---- substitution: the lower half chunks hl-1 .. 0, the upper half
+        // chunks hl .. nch-1, each recomputed from its checkpoint
+        float* colp = reinterpret_cast<float*>(data_) + u;
+        for (int j = 0; j < hu && !failed; ++j) {
+            if (!ready()) { failed = true; break; }
+            if (act && (upper || j < hl)) {
+                const float* t = ring + (size_t)c_buf * 2 * R * W + (upper ? R * W : 0) + col_i;
+                float v[R], g[R];
+#pragma unroll
+                for (int q = 0; q < R; ++q) v[q] = t[q * W];
+                if (!upper) {
+                    const int c = hl - 1 - j, z0 = c * R;
+                    float ee = 0.f, dd = 0.f;
+                    if (c > 0) { const float* k2 = ck + (size_t)(c - 1) * 2 * W + col_i; ee = k2[0]; dd = k2[W]; }
+                    zs_down<true>(zlev, lam, z0, v, g, ee, dd);
+                    float* o = colp + (size_t)(unsigned)(z0 + R - 1) * pl;
+#pragma unroll
+                    for (int q = R - 1; q >= 0; --q) {
+                        x = v[q] - g[q] * x;
+                        *o = x;
+                        o -= pl;
+                    }
+                } else {
+                    const int c = hl + j, z0 = c * R;
+                    float ee = 0.f, dd = 0.f;
+                    float* o = colp + (size_t)(unsigned)z0 * pl;
+                    if (c < nch - 1) {
+                        const float* k2 = ck + (size_t)(c + 1) * 2 * W + col_i;
+                        ee = k2[0];
+                        dd = k2[W];
+                        zs_up<false, true>(zlev, lam, z0, nz, v, g, ee, dd);
+#pragma unroll
+                        for (int q = 0; q < R; ++q) {
+                            x = v[q] - g[q] * x;
+                            *o = x;
+                            o += pl;
+                        }
+                    } else {
+                        zs_up<true, true>(zlev, lam, z0, nz, v, g, ee, dd);
+#pragma unroll
+                        for (int q = 0; q < R; ++q) {
+                            if (z0 + q < nz) {
+                                x = v[q] - g[q] * x;
+                                *o = x;
+                                o += pl;
+                            }
+                        }
+                    }
+                }
+                fsum += x;
+            }
+            release();
+        }
+    }
+    // every consumer arrives here: the loop's named barrier is taken by all
+    // of them or left by all together
+    if (bar_or(1, NC, failed)) {
+        *abort_v = 1;   // the producer stops issuing and waits for its loads
+        return;
+    }
+    if (!isfinite(fsum) && err) atomicOr(err, 1);
+}
+
+// The streamed bulk kernel where it applies (non-periodic z, a field whose
+// rows the tensor map can describe, shared memory for at least three
+// boxes); *used false: the caller takes k_thomas_fast.
+template <bool CPLX>
+cudaError_t launch_stream(void* data, const ZSys& z, const int* skip, int* err, cudaStream_t st, bool* used)
+{
+    using S = ZStream;
+    constexpr int EC = CPLX ? 2 : 1;
+    *used = false;
+    if (z.cyclic || (uintptr_t)data % 16 || (z.plane * EC * sizeof(float)) % 16 || z.plane * EC >= (1L << 31))
+        return cudaSuccess;
+    int dev = 0, sms = 0, optin = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (e != cudaSuccess) return e;
+    const size_t fixed = S::smem(z.nz, 0) + 2 * sizeof(uint64_t) * S::MAX_STAGES + 16;
+    if ((size_t)optin <= fixed) return cudaSuccess;
+    long stages = (long)(((size_t)optin - fixed) / S::STAGE);
+    if (stages > 6) stages = 6;
+    if (stages < 3) return cudaSuccess;
+    CUtensorMap map;
+    if (!tma_map_2d_f32(&map, data, (unsigned long long)z.plane * EC, (unsigned long long)z.nz,
+                        (unsigned long long)z.plane * EC * sizeof(float), (unsigned)S::W, (unsigned)S::R))
+        return cudaSuccess;
+    const size_t smem = S::smem(z.nz, (int)stages);
+    e = cudaFuncSetAttribute(k_thomas_stream<CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const long nblk = (z.plane * EC + S::W - 1) / S::W;
+    const long grid = nblk < sms ? nblk : sms;
+    k_thomas_stream<CPLX><<<(unsigned)grid, S::NT, smem, st>>>(map, data, z, (int)stages, skip, err);
+    *used = true;
+    return cudaGetLastError();
+}
 
 // FP64 z solve of all systems (non-periodic z): thomas_poisson<Exact> with
 // the level coefficients staged once per CTA in shared memory (the same
@@ -724,10 +1143,17 @@ cudaError_t launch_z(float*, const ZSys& z, void* data, const int* skip, int* er
     } else {
         k_thomas_z<float, Exact, CPLX, 2, CYC><<<grid, TPB, 0, lo>>>(data, z, skip, err);
     }
-    if (CYC || !z.ckpt_f || z.plane >= (1L << 31) / 4)
-        k_thomas_z<float, Fast, CPLX, 1, CYC><<<grid, TPB, 0, zs.st>>>(data, z, skip, err);
-    else
-        k_thomas_fast<CPLX><<<grid, TPB, sizeof(float4) * z.nz, zs.st>>>(data, z, skip, err);
+    bool streamed = false;
+    if (!CYC && z.ckpt_f) {
+        const cudaError_t e = launch_stream<CPLX>(data, z, skip, err, zs.st, &streamed);
+        if (e != cudaSuccess) return e;
+    }
+    if (!streamed) {
+        if (CYC || !z.ckpt_f || z.plane >= (1L << 31) / 4)
+            k_thomas_z<float, Fast, CPLX, 1, CYC><<<grid, TPB, 0, zs.st>>>(data, z, skip, err);
+        else
+            k_thomas_fast<CPLX><<<grid, TPB, sizeof(float4) * z.nz, zs.st>>>(data, z, skip, err);
+    }
     if (zs.aux) {
         cudaError_t e = cudaEventRecord(zs.join, zs.aux);
         if (e == cudaSuccess) e = cudaStreamWaitEvent(zs.st, zs.join, 0);
