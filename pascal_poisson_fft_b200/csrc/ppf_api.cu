@@ -96,6 +96,7 @@ double wn_fft(int m, int n, double h)
 struct ppf_plan {
     ppf_desc d{};
     int dev = 0;
+    bool batch_member = false;   // solved beside other problems (ppf_batch): z solve without the streamed kernel
     Geom g{};
     bool xdct = false, ydct = false, cplx = true;
     int ykind = Y_C2C;
@@ -376,6 +377,7 @@ int run_pass(ppf_plan* p, const double* f, double* P, bool resid, bool accumulat
     z.dzmin2 = p->scal;
     z.dc_shift = p->scal + 4;
     z.cyclic = p->g.pz;
+    z.shared_gpu = p->batch_member ? 1 : 0;
     z.ckpt = p->ckpt;
     z.ckpt_f = (sizeof(T) == 4) ? tdma_z_ckpt_f32(p->ckpt, z.nz, z.plane, z.cyclic) : nullptr;
     if (sizeof(T) == 4 && !z.cyclic) {
@@ -1507,6 +1509,7 @@ int batch_init(ppf_batch* b, const ppf_desc* descs, int count, int flags, int br
         if (!p) return fail(PPF_ERR_NOMEM, "host allocation failed");
         b->plans[i] = p;
         p->own_work = false;
+        p->batch_member = true;
         rc = plan_init(p, &descs[i]);
         if (rc != PPF_OK) return rc;
     }

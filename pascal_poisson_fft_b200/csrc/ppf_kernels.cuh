@@ -78,6 +78,7 @@ struct ZSys {
     const double* dzmin2; // device scalar: min_k dx3_k^2 (written by the z-coefficient kernel)
     double* dc_shift;     // device scalar: z-average of the (0,0) solution (subtracted by the y inverse)
     int cyclic;           // periodic z: the reference's cyclic Thomas sequence
+    int shared_gpu;       // other solves run beside this one (a batch): no whole-GPU streamed kernel
     double* ckpt;         // Thomas checkpoints, tdma_z_ckpt_doubles(nz, plane, cyclic, fp32) doubles
     float* ckpt_f;        // FP32 checkpoints of the FP32 bulk kernel (tdma_z_ckpt_f32), or null
     // FP32 storage, non-periodic z: the FP64 low-|k| systems

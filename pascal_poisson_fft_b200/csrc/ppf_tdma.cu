@@ -640,7 +640,8 @@ cudaError_t launch_stream(void* data, const ZSys& z, const int* skip, int* err, 
     using S = ZStream;
     constexpr int EC = CPLX ? 2 : 1;
     *used = false;
-    if (z.cyclic || (uintptr_t)data % 16 || (z.plane * EC * sizeof(float)) % 16 || z.plane * EC >= (1L << 31))
+    if (z.cyclic || z.shared_gpu || (uintptr_t)data % 16 || (z.plane * EC * sizeof(float)) % 16 ||
+        z.plane * EC >= (1L << 31))
         return cudaSuccess;
     int dev = 0, sms = 0, optin = 0;
     cudaError_t e = cudaGetDevice(&dev);
@@ -659,8 +660,13 @@ cudaError_t launch_stream(void* data, const ZSys& z, const int* skip, int* err, 
     const size_t smem = S::smem(z.nz, (int)stages);
     e = cudaFuncSetAttribute(k_thomas_stream<CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
+    // a plane of fewer blocks than SMs leaves most SMs idle behind a few long
+    // chains and fences the others off from concurrent work (batched
+    // problems) with its shared memory: the one-thread-per-system kernel
+    // serves it better
     const long nblk = (z.plane * EC + S::W - 1) / S::W;
-    const long grid = nblk < sms ? nblk : sms;
+    if (nblk < sms) return cudaSuccess;
+    const long grid = sms;
     k_thomas_stream<CPLX><<<(unsigned)grid, S::NT, smem, st>>>(map, data, z, (int)stages, skip, err);
     *used = true;
     return cudaGetLastError();
