@@ -254,12 +254,29 @@ __device__ __forceinline__ void fft_tile(cx<T>* s, const FftSched& sch, int W, i
 // are template parameters, so every index, division and loop bound is a
 // constant.  Same layout and pass structure as fft_tile.
 // ---------------------------------------------------------------------------
-template <typename T, int W>
+// Tiles of length N whose rows are half a 128-byte bank row (W complex
+// values of 64 bytes) and whose first pass is radix 8: that pass stores
+// rows 8 apart and the position-fastest last pass reads 32 consecutive
+// rows, which in the plain layout fall on one half of the bank rows; row n
+// trades places with row n ^ 1 when bit 3 of n is set, which spreads both
+// over the two halves.  (N is a multiple of 16, so every row has its
+// partner; a row N past the end, the pipelines' extra Nyquist row, has
+// bit 3 clear.)  Used where shared-memory throughput bounds the kernel, the
+// FP64 512-point y pipeline (y passes 0.462 -> 0.450 ms per FP64 solve);
+// the FP32 256-point x tiles, issue-bound, lose more to the three integer
+// instructions per access than they gain (x passes +5-8 %).
+template <typename T, int W, int N>
+struct HalfRowSwap {
+    static constexpr bool value = W * (int)sizeof(cx<T>) == 64 && sizeof(T) == 8 && N == 512;
+};
+
+template <typename T, int W, int N = 0>
 __device__ __forceinline__ int sidx_ct(int n, int l)
 {
     constexpr int G = SwizzleG<T>::value;
     constexpr int MASK = (W < G ? W : G) - 1;
-    return n * W + (l ^ (n & MASK));
+    const int m = HalfRowSwap<T, W, N>::value ? (n ^ ((n >> 3) & 1)) : n;
+    return m * W + (l ^ (n & MASK));
 }
 
 // Marker loader and storer of fft_pass_ct: the pass reads its inputs from
@@ -290,7 +307,7 @@ __device__ __forceinline__ void fft_pass_ct(cx<T>* s, const cx<T>* __restrict__ 
             const int l = JF ? t / NB : t % W, j = JF ? t % NB : t / W;
 #pragma unroll
             for (int r = 0; r < R; ++r) {
-                if constexpr (std::is_same<LD, TileLd>::value) v[q * R + r] = s[sidx_ct<T, W>(j + r * NB, l)];
+                if constexpr (std::is_same<LD, TileLd>::value) v[q * R + r] = s[sidx_ct<T, W, N>(j + r * NB, l)];
                 else v[q * R + r] = ld(j + r * NB, l);
             }
         }
@@ -307,7 +324,7 @@ __device__ __forceinline__ void fft_pass_ct(cx<T>* s, const cx<T>* __restrict__ 
             const int base = (j - k) * R + k;
 #pragma unroll
             for (int r = 0; r < R; ++r) {
-                if constexpr (std::is_same<ST, TileSt>::value) s[sidx_ct<T, W>(base + r * NS, l)] = v[q * R + r];
+                if constexpr (std::is_same<ST, TileSt>::value) s[sidx_ct<T, W, N>(base + r * NS, l)] = v[q * R + r];
                 else st(base + r * NS, l, v[q * R + r]);
             }
         }
@@ -386,5 +403,14 @@ struct ShapeCT {
         fft_ct_chain<T, INV, N_, W_, NT_, 1, true, LD, ST, RS...>(s, tw, ld, st);
     }
 };
+
+// The element (n, l) of a tile of shape SH: the compile-time layout of a
+// compile-time shape (the one its FFT passes use), else sidx.
+template <typename T, typename SH>
+__device__ __forceinline__ int tidx(int n, int l, int W)
+{
+    if constexpr (SH::CT) return sidx_ct<T, SH::W, SH::N>(n, l);
+    else return sidx<T>(n, l, W);
+}
 
 }  // namespace ppf

@@ -100,7 +100,7 @@ __global__ void __launch_bounds__(SH::NT, (SH::N == 384 || SH::N <= 128) ? 2 : 0
         const long line0 = t * W;
         for (int e = threadIdx.x; e < ER; e += NT) {
             const int l = e / NR, k = e - l * NR;
-            cx<T>* d = b + sidx_ct<T, W>(k, l);
+            cx<T>* d = b + sidx_ct<T, W, SH::N>(k, l);
             if (line0 + l < nlines) cp_async_elem(d, in + (line0 + l) * in_pitch + k);
             else *d = mk<T>((T)0, (T)0);
         }
@@ -146,8 +146,8 @@ __global__ void __launch_bounds__(SH::NT, (SH::N == 384 || SH::N <= 128) ? 2 : 0
         // first FFT pass loads its inputs (X_0 and X_nc enter with zero
         // imaginary parts)
         auto zsplit = [&](int m, int l) -> cx<T> {
-            cx<T> a = cur[sidx_ct<T, W>(m, l)];
-            cx<T> xc = cur[sidx_ct<T, W>(NC - m, l)];
+            cx<T> a = cur[sidx_ct<T, W, SH::N>(m, l)];
+            cx<T> xc = cur[sidx_ct<T, W, SH::N>(NC - m, l)];
             if (m == 0) { a.y = (T)0; xc.y = (T)0; }
             const cx<T> b = conj(xc);
             const cx<T> Ev = a + b, D = a - b;

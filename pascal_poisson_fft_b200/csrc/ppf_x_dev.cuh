@@ -161,7 +161,7 @@ __device__ __forceinline__ void xfwd(const double* __restrict__ f, const ResidIn
             }
             z = mk<T>((T)a, (T)b);
         }
-        s[sidx<T>(n, l, W)] = z;
+        s[tidx<T, SH>(n, l, W)] = z;
     }
     __syncthreads();
 
@@ -177,8 +177,8 @@ __device__ __forceinline__ void xfwd(const double* __restrict__ f, const ResidIn
             if (e < E) {
                 const int l = e / nc, m = e - l * nc;
                 const int q0 = 2 * m, q1 = 2 * m + 1;
-                const T v0 = (q0 < nc) ? s[sidx<T>(q0, l, W)].x : s[sidx<T>(nx - 1 - q0, l, W)].y;
-                const T v1 = (q1 < nc) ? s[sidx<T>(q1, l, W)].x : s[sidx<T>(nx - 1 - q1, l, W)].y;
+                const T v0 = (q0 < nc) ? s[tidx<T, SH>(q0, l, W)].x : s[tidx<T, SH>(nx - 1 - q0, l, W)].y;
+                const T v1 = (q1 < nc) ? s[tidx<T, SH>(q1, l, W)].x : s[tidx<T, SH>(nx - 1 - q1, l, W)].y;
                 tmp[i] = mk<T>(v0, v1);
             }
         }
@@ -188,7 +188,7 @@ __device__ __forceinline__ void xfwd(const double* __restrict__ f, const ResidIn
             const int e = threadIdx.x + i * NTH;
             if (e < E) {
                 const int l = e / nc, m = e - l * nc;
-                s[sidx<T>(m, l, W)] = tmp[i];
+                s[tidx<T, SH>(m, l, W)] = tmp[i];
             }
         }
         __syncthreads();
@@ -205,8 +205,8 @@ __device__ __forceinline__ void xfwd(const double* __restrict__ f, const ResidIn
             const long line = line0 + l;
             if (line >= nlines) continue;
             const int kc = nc - k;
-            const cx<T> a = s[sidx<T>(k, l, W)];
-            const cx<T> b = s[sidx<T>(k == 0 ? 0 : kc, l, W)];
+            const cx<T> a = s[tidx<T, SH>(k, l, W)];
+            const cx<T> b = s[tidx<T, SH>(k == 0 ? 0 : kc, l, W)];
             cx<T>* orow = out + line * out_pitch;
             {
                 const cx<T> zc = conj(b);
@@ -233,8 +233,8 @@ __device__ __forceinline__ void xfwd(const double* __restrict__ f, const ResidIn
             const long line = line0 + l;
             if (line >= nlines) continue;
             const int kap = (k <= nc) ? k : nx - k;
-            const cx<T> zk = s[sidx<T>(kap == nc ? 0 : kap, l, W)];
-            const cx<T> zc = conj(s[sidx<T>(kap == 0 ? 0 : nc - kap, l, W)]);
+            const cx<T> zk = s[tidx<T, SH>(kap == nc ? 0 : kap, l, W)];
+            const cx<T> zc = conj(s[tidx<T, SH>(kap == 0 ? 0 : nc - kap, l, W)]);
             const cx<T> Ev = (zk + zc) * (T)0.5;
             const cx<T> D = zk - zc;
             const cx<T> O = mk<T>(D.y * (T)0.5, -D.x * (T)0.5);
@@ -339,8 +339,8 @@ __device__ __forceinline__ void xinv(const void* __restrict__ in_, long in_pitch
                     Zc = mk<T>(Ev.x - O.y, Ev.y + O.x);
                 }
             }
-            s[sidx<T>(k, l, W)] = Zk;
-            if (k != 0 && kc != k) s[sidx<T>(kc, l, W)] = Zc;
+            s[tidx<T, SH>(k, l, W)] = Zk;
+            if (k != 0 && kc != k) s[tidx<T, SH>(kc, l, W)] = Zc;
         }
     } else
     for (int e = threadIdx.x; e < E; e += NTH) {
@@ -371,7 +371,7 @@ __device__ __forceinline__ void xinv(const void* __restrict__ in_, long in_pitch
             const cx<T> O = cmul(D, conj(ldg(tw_n + k)));
             Z = mk<T>(Ev.x - O.y, Ev.y + O.x);
         }
-        s[sidx<T>(k, l, W)] = Z;
+        s[tidx<T, SH>(k, l, W)] = Z;
     }
     // ghosted-output offset of each line of the tile, and (GHOST) the offsets
     // of the ghost lines its values are copied to (0: none)
@@ -409,7 +409,7 @@ __device__ __forceinline__ void xinv(const void* __restrict__ in_, long in_pitch
         for (int e = threadIdx.x; e < E; e += NTH) {
             const int l = e / nc, n = e - l * nc;
             if (line0 + l >= nlines) continue;
-            const cx<T> zv = s[sidx<T>(n, l, W)];
+            const cx<T> zv = s[tidx<T, SH>(n, l, W)];
             const double x0 = (double)zv.x, x1 = (double)zv.y;
             const long o = line_base[l] + 2 * n;
             // refinement: u <- u + du - mean(u), the FP64 mean of the previous
@@ -445,7 +445,7 @@ __device__ __forceinline__ void xinv(const void* __restrict__ in_, long in_pitch
             int n = i;
             // inverse Makhoul order (cuda_Poisson_DCT_b_post, :1013-1033)
             if (DCT) n = (i & 1) ? (nc + ((nx - 1 - i) >> 1)) : (i >> 1);
-            const cx<T> zv = s[sidx<T>(n >> 1, l, W)];
+            const cx<T> zv = s[tidx<T, SH>(n >> 1, l, W)];
             const double x = (double)((n & 1) ? zv.y : zv.x);
             const long o = line_base[l] + i;
             // refinement: u <- u + du - mean(u), the FP64 mean of the previous

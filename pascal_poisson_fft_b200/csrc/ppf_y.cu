@@ -62,7 +62,7 @@ __device__ __forceinline__ void y_c2c_pipe(const cx<T>* __restrict__ in, long in
         for (int i = 0; i < EPT; ++i) {
             const int e = threadIdx.x + i * NT;
             const int l = e & (W - 1), y = e >> LGW;
-            cx<T>* d = b + sidx_ct<T, W>(y, l);
+            cx<T>* d = b + sidx_ct<T, W, SH::N>(y, l);
             if (col0 + l < ncols) cp_async_elem(d, inp + (long)y * in_pitch + l);
             else *d = mk<T>((T)0, (T)0);
         }
@@ -78,7 +78,7 @@ __device__ __forceinline__ void y_c2c_pipe(const cx<T>* __restrict__ in, long in
         const int z = (int)(t / nblk), col0 = (int)(t - (long)z * nblk) * W;
         // the zero mode's z-average, removed from the (kx,ky) = (0,0) coefficient
         // (element (0,0) is copied by thread 0)
-        if (INV && dc_shift && col0 == 0 && threadIdx.x == 0) cur[sidx_ct<T, W>(0, 0)].x -= (T)*dc_shift;
+        if (INV && dc_shift && col0 == 0 && threadIdx.x == 0) cur[sidx_ct<T, W, SH::N>(0, 0)].x -= (T)*dc_shift;
         __syncthreads();
         // the last pass stores the tile's rows straight to the output (a warp
         // writes whole W-column row segments, as a copy-out loop would); the

@@ -42,7 +42,7 @@ __device__ __forceinline__ void yfwd(const cx<T>* __restrict__ in, long in_pitch
         if (col < ncols) v = inp[(long)y * in_pitch + col];
         int row = y;
         if (KIND == Y_CDCT) row = (y & 1) ? (ny - 1 - (y >> 1)) : (y >> 1);
-        s[sidx<T>(row, l, W)] = v;
+        s[tidx<T, SH>(row, l, W)] = v;
     }
     __syncthreads();
     tile_fft<T, false, SH>(s, sch, W, lgW, tw_ny);
@@ -52,7 +52,7 @@ __device__ __forceinline__ void yfwd(const cx<T>* __restrict__ in, long in_pitch
         for (int e = threadIdx.x; e < E; e += NTH) {
             const int l = e & (W - 1), k = e >> lgW;
             const int col = col0 + l;
-            if (col < ncols) outp[(long)k * out_pitch + col] = s[sidx<T>(k, l, W)];
+            if (col < ncols) outp[(long)k * out_pitch + col] = s[tidx<T, SH>(k, l, W)];
         }
     } else if (KIND == Y_CDCT) {
         cx<T>* outp = out + (long)z * ny * out_pitch;
@@ -60,8 +60,8 @@ __device__ __forceinline__ void yfwd(const cx<T>* __restrict__ in, long in_pitch
             const int l = e & (W - 1), k = e >> lgW;
             const int col = col0 + l;
             if (col >= ncols) continue;
-            const cx<T> V = s[sidx<T>(k, l, W)];
-            const cx<T> Vp = s[sidx<T>(k == 0 ? 0 : ny - k, l, W)];
+            const cx<T> V = s[tidx<T, SH>(k, l, W)];
+            const cx<T> Vp = s[tidx<T, SH>(k == 0 ? 0 : ny - k, l, W)];
             const cx<T> w = ldg(tw_dct + k);
             cx<T> X;
             X.x = w.x * (V.x + Vp.x) - w.y * (V.y - Vp.y);
@@ -76,8 +76,8 @@ __device__ __forceinline__ void yfwd(const cx<T>* __restrict__ in, long in_pitch
             const int l = e & (W - 1), k = e >> lgW;
             const int col = col0 + l;
             if (col >= ncols) continue;
-            const cx<T> zk = s[sidx<T>(k == ny ? 0 : k, l, W)];
-            const cx<T> zc = conj(s[sidx<T>(k == 0 ? 0 : ny - k, l, W)]);
+            const cx<T> zk = s[tidx<T, SH>(k == ny ? 0 : k, l, W)];
+            const cx<T> zc = conj(s[tidx<T, SH>(k == 0 ? 0 : ny - k, l, W)]);
             const cx<T> X1 = (zk + zc) * (T)0.5;
             const cx<T> D = zk - zc;
             const cx<T> X2 = mk<T>(D.y * (T)0.5, -D.x * (T)0.5);
@@ -115,7 +115,7 @@ __device__ __forceinline__ void yinv(const cx<T>* __restrict__ in, long in_pitch
             cx<T> v = mk<T>((T)0, (T)0);
             if (col < ncols) v = inp[(long)k * in_pitch + col];
             if (k == 0 && col == 0) v.x -= shift;
-            s[sidx<T>(k, l, W)] = v;
+            s[tidx<T, SH>(k, l, W)] = v;
         }
     } else if (KIND == Y_CDCT) {
         // Z_k = e^{i pi k/(2n)} (X_k - i X_{n-k}) per real component
@@ -136,7 +136,7 @@ __device__ __forceinline__ void yinv(const cx<T>* __restrict__ in, long in_pitch
                 const T zbx = c * X.y + sn * Xp.y, zby = sn * X.y - c * Xp.y;
                 Z = mk<T>(zax - zby, zay + zbx);
             }
-            s[sidx<T>(k, l, W)] = Z;
+            s[tidx<T, SH>(k, l, W)] = Z;
         }
     } else {
         const int my = ny / 2 + 1;
@@ -154,7 +154,7 @@ __device__ __forceinline__ void yinv(const cx<T>* __restrict__ in, long in_pitch
                 if (k == 0 && col == 0) X1.x -= shift;
                 Z = mk<T>(X1.x - X2.y, X1.y + X2.x);
             }
-            s[sidx<T>(k, l, W)] = Z;
+            s[tidx<T, SH>(k, l, W)] = Z;
         }
     }
     __syncthreads();
@@ -168,7 +168,7 @@ __device__ __forceinline__ void yinv(const cx<T>* __restrict__ in, long in_pitch
         int n = i;
         // inverse Makhoul order (cuda_Poisson_DCT_b_post, :1013-1033)
         if (KIND == Y_CDCT) n = (i & 1) ? (ny / 2 + ((ny - 1 - i) >> 1)) : (i >> 1);
-        outp[(long)i * out_pitch + col] = s[sidx<T>(n, l, W)];
+        outp[(long)i * out_pitch + col] = s[tidx<T, SH>(n, l, W)];
     }
 }
 
