@@ -74,6 +74,12 @@ __device__ __forceinline__ void cp_async_elem(cx<double>* dst, const cx<double>*
     const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
 }
+// 16 bytes, both addresses 16-byte aligned
+__device__ __forceinline__ void cp_async_16(void* dst, const void* src)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 // wait until at most N of this thread's most recent groups are pending
 template <int N>

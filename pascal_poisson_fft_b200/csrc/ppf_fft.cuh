@@ -162,20 +162,27 @@ template <typename T, bool INV> struct Dft<T, INV, 16> {
 // FP32, which the FP64 refinement absorbs): one load instead of R-1 in the
 // passes the FP32 y kernels are bound by.
 template <typename T, bool INV, int R>
+__device__ __forceinline__ void twiddle_powers(cx<T>* w, const cx<T>* __restrict__ tw, int k, int ts)
+{
+    static_assert(sizeof(T) == 4 && (R == 4 || R == 5 || R == 8), "FP32 radix 4, 5 or 8");
+    w[1] = ldg(tw + k * ts);
+    if (INV) w[1].y = -w[1].y;
+    w[2] = cmul(w[1], w[1]);
+    w[3] = cmul(w[1], w[2]);
+    if constexpr (R >= 5) w[4] = cmul(w[2], w[2]);
+    if constexpr (R == 8) {
+        w[5] = cmul(w[4], w[1]);
+        w[6] = cmul(w[4], w[2]);
+        w[7] = cmul(w[4], w[3]);
+    }
+}
+
+template <typename T, bool INV, int R>
 __device__ __forceinline__ void twiddle_mul(cx<T>* v, const cx<T>* __restrict__ tw, int k, int ts)
 {
     if constexpr (sizeof(T) == 4 && (R == 4 || R == 5 || R == 8)) {
         cx<T> w[R];
-        w[1] = ldg(tw + k * ts);
-        if (INV) w[1].y = -w[1].y;
-        w[2] = cmul(w[1], w[1]);
-        w[3] = cmul(w[1], w[2]);
-        if constexpr (R >= 5) w[4] = cmul(w[2], w[2]);
-        if constexpr (R == 8) {
-            w[5] = cmul(w[4], w[1]);
-            w[6] = cmul(w[4], w[2]);
-            w[7] = cmul(w[4], w[3]);
-        }
+        twiddle_powers<T, INV, R>(w, tw, k, ts);
 #pragma unroll
         for (int r = 1; r < R; ++r) v[r] = cmul(v[r], w[r]);
     } else {
@@ -369,6 +376,90 @@ __device__ __forceinline__ void fft_ct_last_st(cx<T>* s, const cx<T>* __restrict
     }
 }
 
+// ---------------------------------------------------------------------------
+// Paired passes: FP32 tiles of 16 lines, whose rows are one 128-byte bank
+// row.  A thread takes the butterflies of lines 2p and 2p + 1 at one
+// position, so one 16-byte shared access moves the values of both lines and
+// one set of twiddle powers serves both (the same operations per line as
+// fft_pass_ct).  Element (n, l) sits at n * 16 + l, unswizzled: a warp's
+// accesses cover four whole rows, which is free of bank conflicts.
+// ---------------------------------------------------------------------------
+constexpr int PAIR_W = 16;
+
+template <bool INV, int N, int NT, int R, int NS, typename ST = TileSt>
+__device__ __forceinline__ void fft_pass_pair(cx<float>* s, const cx<float>* __restrict__ tw, ST st = ST{})
+{
+    constexpr int P = PAIR_W / 2;
+    constexpr int NB = N / R;
+    constexpr int ITEMS = NB * P;
+    constexpr int Q = (ITEMS + NT - 1) / NT;
+    constexpr int TS = N / (NS * R);
+    float4* s4 = reinterpret_cast<float4*>(s);
+    cx<float> a[Q * R], b[Q * R];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        const int t = threadIdx.x + q * NT;
+        if (ITEMS % NT == 0 || t < ITEMS) {
+            const int p = t % P, j = t / P;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const float4 f = s4[(j + r * NB) * P + p];
+                a[q * R + r] = mk(f.x, f.y);
+                b[q * R + r] = mk(f.z, f.w);
+            }
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        const int t = threadIdx.x + q * NT;
+        if (ITEMS % NT == 0 || t < ITEMS) {
+            const int p = t % P, j = t / P;
+            const int k = j % NS;
+            if constexpr (NS > 1) {
+                cx<float> w[R];
+                if constexpr (R == 4 || R == 5 || R == 8) {
+                    twiddle_powers<float, INV, R>(w, tw, k, TS);
+                } else {
+#pragma unroll
+                    for (int r = 1; r < R; ++r) {
+                        w[r] = ldg(tw + r * k * TS);
+                        if (INV) w[r].y = -w[r].y;
+                    }
+                }
+#pragma unroll
+                for (int r = 1; r < R; ++r) {
+                    a[q * R + r] = cmul(a[q * R + r], w[r]);
+                    b[q * R + r] = cmul(b[q * R + r], w[r]);
+                }
+            }
+            Dft<float, INV, R>::run(a + q * R);
+            Dft<float, INV, R>::run(b + q * R);
+            const int base = (j - k) * R + k;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const cx<float> u = a[q * R + r], v = b[q * R + r];
+                if constexpr (std::is_same<ST, TileSt>::value) s4[(base + r * NS) * P + p] = make_float4(u.x, u.y, v.x, v.y);
+                else st(base + r * NS, p, u, v);
+            }
+        }
+    }
+    __syncthreads();
+}
+
+// Every paired pass of a radix sequence, the last one handing outputs n of
+// lines 2p and 2p + 1 to st(n, p, u, v) instead of the tile
+template <bool INV, int N, int NT, int NS, typename ST, int R0, int... RS>
+__device__ __forceinline__ void fft_pair_last_st(cx<float>* s, const cx<float>* __restrict__ tw, ST st)
+{
+    if constexpr (sizeof...(RS) == 0) {
+        fft_pass_pair<INV, N, NT, R0, NS, ST>(s, tw, st);
+    } else {
+        fft_pass_pair<INV, N, NT, R0, NS>(s, tw);
+        fft_pair_last_st<INV, N, NT, NS * R0, ST, RS...>(s, tw, st);
+    }
+}
+
 // Tile shapes.  ShapeRT: everything at run time (fft_tile).  ShapeCT: a
 // fixed length N = product of RS, W lines, NT threads per CTA.
 struct ShapeRT {
@@ -401,6 +492,14 @@ struct ShapeCT {
     static __device__ __forceinline__ void fft_ld_st(cx<T>* s, const cx<T>* __restrict__ tw, LD ld, ST st)
     {
         fft_ct_chain<T, INV, N_, W_, NT_, 1, true, LD, ST, RS...>(s, tw, ld, st);
+    }
+    // fft_st in paired passes (FP32, W = PAIR_W): st(n, p, u, v) receives
+    // outputs n of lines 2p and 2p + 1
+    template <bool INV, typename ST>
+    static __device__ __forceinline__ void fft_pair_st(cx<float>* s, const cx<float>* __restrict__ tw, ST st)
+    {
+        static_assert(W_ == PAIR_W, "paired passes take 16-line tiles");
+        fft_pair_last_st<INV, N_, NT_, 1, ST, RS...>(s, tw, st);
     }
 };
 

@@ -40,7 +40,11 @@ __global__ void __launch_bounds__(512) k_yinv(const cx<T>* __restrict__ in, long
 // are copied into the second buffer with cp.async while the current tile
 // is transformed and stored, so the loads of one tile overlap the
 // butterflies of the previous one.
-template <typename T, bool INV, typename SH>
+//
+// PAIR (FP32 tiles of 16 columns, 16-byte aligned rows): the tile is
+// unswizzled, copied in 16-byte pairs of columns, and transformed by the
+// paired passes (fft_pass_pair), which also store column pairs.
+template <typename T, bool INV, typename SH, bool PAIR>
 __device__ __forceinline__ void y_c2c_pipe(const cx<T>* __restrict__ in, long in_pitch, cx<T>* __restrict__ out,
                                            long out_pitch, int ncols, int nz, const cx<T>* __restrict__ tw,
                                            const double* __restrict__ dc_shift, const int* __restrict__ skip)
@@ -50,6 +54,7 @@ __device__ __forceinline__ void y_c2c_pipe(const cx<T>* __restrict__ in, long in
     constexpr int LGW = ct_log2y(W);
     constexpr int EPT = (N * W) / NT;
     static_assert(EPT * NT == N * W, "tile elements must divide over the threads");
+    static_assert(!PAIR || (sizeof(T) == 4 && W == PAIR_W && EPT % 2 == 0), "paired tiles: FP32, 16 columns");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cx<T>* cur = reinterpret_cast<cx<T>*>(smem_raw);
     cx<T>* nxt = cur + N * W;
@@ -58,13 +63,32 @@ __device__ __forceinline__ void y_c2c_pipe(const cx<T>* __restrict__ in, long in
     auto issue = [&](long t, cx<T>* b) {
         const int z = (int)(t / nblk), col0 = (int)(t - (long)z * nblk) * W;
         const cx<T>* inp = in + (long)z * N * in_pitch + col0;
+        if constexpr (PAIR) {
+            constexpr int P = W / 2;
 #pragma unroll
-        for (int i = 0; i < EPT; ++i) {
-            const int e = threadIdx.x + i * NT;
-            const int l = e & (W - 1), y = e >> LGW;
-            cx<T>* d = b + sidx_ct<T, W, SH::N>(y, l);
-            if (col0 + l < ncols) cp_async_elem(d, inp + (long)y * in_pitch + l);
-            else *d = mk<T>((T)0, (T)0);
+            for (int i = 0; i < EPT / 2; ++i) {
+                const int e = threadIdx.x + i * NT;
+                const int p = e % P, y = e / P;
+                cx<T>* d = b + y * W + 2 * p;
+                const cx<T>* src = inp + (long)y * in_pitch + 2 * p;
+                const int c = col0 + 2 * p;
+                if (c + 1 < ncols) {
+                    cp_async_16(d, src);
+                } else {
+                    if (c < ncols) cp_async_elem(d, src);
+                    else d[0] = mk<T>((T)0, (T)0);
+                    d[1] = mk<T>((T)0, (T)0);
+                }
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < EPT; ++i) {
+                const int e = threadIdx.x + i * NT;
+                const int l = e & (W - 1), y = e >> LGW;
+                cx<T>* d = b + sidx_ct<T, W, SH::N>(y, l);
+                if (col0 + l < ncols) cp_async_elem(d, inp + (long)y * in_pitch + l);
+                else *d = mk<T>((T)0, (T)0);
+            }
         }
         cp_async_commit();
     };
@@ -84,10 +108,20 @@ __device__ __forceinline__ void y_c2c_pipe(const cx<T>* __restrict__ in, long in
         // writes whole W-column row segments, as a copy-out loop would); the
         // tile is free for the refill two tiles on when the transform returns
         cx<T>* outp = out + (long)z * N * out_pitch + col0;
-        auto yst = [&](int k, int l, cx<T> v) {
-            if (col0 + l < ncols) outp[(long)k * out_pitch + l] = v;
-        };
-        SH::template fft_st<T, INV>(cur, tw, yst);
+        if constexpr (PAIR) {
+            auto yst2 = [&](int k, int p, cx<T> u, cx<T> v) {
+                cx<T>* o = outp + (long)k * out_pitch + 2 * p;
+                const int c = col0 + 2 * p;
+                if (c + 1 < ncols) *reinterpret_cast<float4*>(o) = make_float4(u.x, u.y, v.x, v.y);
+                else if (c < ncols) *o = u;
+            };
+            SH::template fft_pair_st<INV>(cur, tw, yst2);
+        } else {
+            auto yst = [&](int k, int l, cx<T> v) {
+                if (col0 + l < ncols) outp[(long)k * out_pitch + l] = v;
+            };
+            SH::template fft_st<T, INV>(cur, tw, yst);
+        }
         cx<T>* tmp = cur;
         cur = nxt;
         nxt = tmp;
@@ -95,14 +129,14 @@ __device__ __forceinline__ void y_c2c_pipe(const cx<T>* __restrict__ in, long in
 }
 
 // FP32 tiles: one CTA per SM (two 64 KB buffers at 512 threads)
-template <typename T, bool INV, typename SH>
+template <typename T, bool INV, typename SH, bool PAIR>
 __global__ void __launch_bounds__(SH::NT) k_y_c2c_pipe(const cx<T>* __restrict__ in, long in_pitch,
                                                       cx<T>* __restrict__ out, long out_pitch, int ncols, int nz,
                                                       const cx<T>* __restrict__ tw,
                                                       const double* __restrict__ dc_shift,
                                                       const int* __restrict__ skip)
 {
-    y_c2c_pipe<T, INV, SH>(in, in_pitch, out, out_pitch, ncols, nz, tw, dc_shift, skip);
+    y_c2c_pipe<T, INV, SH, PAIR>(in, in_pitch, out, out_pitch, ncols, nz, tw, dc_shift, skip);
 }
 
 // FP64 tiles (half width, 256 threads): three resident CTAs per SM, which
@@ -114,7 +148,7 @@ __global__ void __launch_bounds__(SH::NT, 3) k_y_c2c_pipe64(const cx<double>* __
                                                            const double* __restrict__ dc_shift,
                                                            const int* __restrict__ skip)
 {
-    y_c2c_pipe<double, INV, SH>(in, in_pitch, out, out_pitch, ncols, nz, tw, dc_shift, skip);
+    y_c2c_pipe<double, INV, SH, false>(in, in_pitch, out, out_pitch, ncols, nz, tw, dc_shift, skip);
 }
 
 // Tile shape of the pipelined y kernel.  FP64 tiles of 512-thread shapes
@@ -133,9 +167,15 @@ template <typename T, bool INV, typename SH>
 cudaError_t launch_y_c2c_pipe(const cx<T>* in, long in_pitch, cx<T>* out, long out_pitch, int ncols, int nz,
                               const cx<T>* tw, const double* dc_shift, const int* skip_flag, cudaStream_t st)
 {
-    auto kern = [] {
+    // paired passes where the tile is 16 FP32 columns and every column pair
+    // starts on a 16-byte boundary
+    constexpr bool PAIRABLE = sizeof(T) == 4 && SH::W == PAIR_W;
+    const bool pair = PAIRABLE && in_pitch % 2 == 0 && out_pitch % 2 == 0 && ((uintptr_t)in & 15) == 0 &&
+                      ((uintptr_t)out & 15) == 0;
+    auto kern = [&] {
         if constexpr (sizeof(T) == 8) return k_y_c2c_pipe64<INV, SH>;
-        else return k_y_c2c_pipe<T, INV, SH>;
+        else if constexpr (PAIRABLE) return pair ? k_y_c2c_pipe<T, INV, SH, true> : k_y_c2c_pipe<T, INV, SH, false>;
+        else return k_y_c2c_pipe<T, INV, SH, false>;
     }();
     const size_t smem = 2 * (size_t)SH::N * SH::W * sizeof(cx<T>);
     cudaError_t e = set_smem(kern, smem);
