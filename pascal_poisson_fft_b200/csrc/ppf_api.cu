@@ -418,7 +418,7 @@ int run_pass(ppf_plan* p, const double* f, double* P, bool resid, bool accumulat
     // the mixed path keeps the stencil's ghost cells current for its residual
     long nblk = 0;
     e = launch_xinv<T>(p->xdct, p->A, p->a_pitch, P, p->U, uk, p->g, accumulate, p->d.precision == PPF_MIXED,
-                       p->partials, p->scal + 5, p->sx, txh, txn, txd, skip, st, &nblk);
+                       p->partials, p->scal + 5, p->sx, txh, txn, txd, skip, st, &nblk, p->flags + 2);
     if (p->partials) p->xinv_nblk = nblk;  // the refinement gate reduces these blocks' partial sums
     if (e != cudaSuccess) return cuda_fail(e, "x inverse");
     mark(p, 5, st);

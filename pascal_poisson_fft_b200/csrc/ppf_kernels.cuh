@@ -56,7 +56,7 @@ template <typename T>
 cudaError_t launch_xinv(bool dct, const void* in, long in_pitch, double* P, float* U, int ukind, const Geom& g,
                         bool accumulate, bool stencil_ghosts, double* partials, const double* mean_prev,
                         const FftSched& sch, const cx<T>* tw_half, const cx<T>* tw_n, const cx<T>* tw_dct,
-                        const int* skip_flag, cudaStream_t st, long* blocks_used = nullptr);
+                        const int* skip_flag, cudaStream_t st, long* blocks_used = nullptr, int* err = nullptr);
 
 // upper bound of the blocks launch_xinv uses for geometry g (one per tile;
 // size of the partials array / 3); the launch reports the blocks it used

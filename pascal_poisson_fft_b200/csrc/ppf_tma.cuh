@@ -1,7 +1,7 @@
-// ppf_tma.cuh -- tensor-memory-access (TMA) tile loads into shared memory
-// with completion on an mbarrier (sm_100a PTX), and the host-side encoding
-// of their tensor maps.  Loads only, never with cluster multicast: every
-// map describes this GPU's own memory.
+// ppf_tma.cuh -- tensor-memory-access (TMA) tile and bulk loads into shared
+// memory with completion on an mbarrier (sm_100a PTX), and the host-side
+// encoding of their tensor maps.  Loads only, never with cluster multicast:
+// every source is this GPU's own memory.
 #pragma once
 #include <cuda.h>
 #include <cuda_runtime.h>
@@ -106,6 +106,16 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, i
         " [%0], [%1, {%2, %3}], [%4], %5;\n" ::"r"(smem_u32(dst)),
         "l"(map), "r"(x), "r"(y), "r"(smem_u32(bar)), "l"(policy)
         : "memory");
+}
+
+// `bytes` (a multiple of 16) from global src to shared dst, both 16-byte
+// aligned, completing on bar (a bulk copy of consecutive bytes)
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, uint64_t* bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
 }
 
 // Order this CTA's earlier generic-proxy accesses of shared memory before

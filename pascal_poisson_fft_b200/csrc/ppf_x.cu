@@ -8,9 +8,18 @@
 // passes (01_Fortran/src/fft_3d_poisson.f90:378-419, 561-616, 915-1033);
 // here each is one read and one write of the field.  SH selects the
 // compile-time engine of a common length or the run-time engine.
+#include "ppf_tma.cuh"
 #include "ppf_x_dev.cuh"
 
 #include <type_traits>
+
+#ifndef PPF_XINV_BULK
+#define PPF_XINV_BULK 1
+#endif
+// resident CTAs per SM asked of the 256-point x-inverse pipeline (a register bound)
+#ifndef PPF_XINV_256_CTAS
+#define PPF_XINV_256_CTAS 5
+#endif
 
 namespace ppf {
 
@@ -67,27 +76,55 @@ __global__ void __launch_bounds__(SH::NT, 5) k_xinv64(PPF_XINV_PARAMS)
 // first FFT pass loads its inputs, and the last pass hands its outputs to
 // the accumulate and store -- the output semantics of
 // k_xinv<T, false, ACC, GHOST, SH, UK>.  (FP64 tiles take the non-pipelined kernel:
-// two 66 KB buffers at 128 registers leave too few resident CTAs.)
+// two 66 KB buffers at 128 registers leave too few resident CTAs.)  BULK:
+// each line's spectral row arrives as one bulk copy (cp.async.bulk, one
+// thread, completion on an mbarrier per buffer) into a raw buffer of rows
+// XINV_RS(NC) values apart, instead of one cp.async per value: rows of
+// NC + 2 values (16-byte multiples), which the row pitch must hold; the row
+// stride is 4 mod 16 values, so the split's line-fastest reads spread over
+// the banks.  A wait that gives up (about 2 s of sleeping polls) sets err
+// bit 2 and ends the CTA's walk.
 // --------------------------------------------------------------------------
-template <typename T, bool ACC, bool GHOST, typename SH, int UK = U_P>
-__global__ void __launch_bounds__(SH::NT, (SH::N == 384 || SH::N <= 128) ? 2 : 0) k_xinv_pipe(const cx<T>* __restrict__ in, long in_pitch,
+constexpr int xinv_rs(int nc) { return ((nc + 2 + 11) / 16) * 16 + 4; }
+constexpr unsigned XB_POLL_NS = 20000;
+constexpr long XB_WAIT_LIMIT = 100000;
+
+template <typename T, bool ACC, bool GHOST, typename SH, int UK = U_P, bool BULK = false>
+__global__ void __launch_bounds__(SH::NT, (SH::N == 384 || SH::N <= 128) ? 2 : (SH::N == 256 ? PPF_XINV_256_CTAS : 0)) k_xinv_pipe(const cx<T>* __restrict__ in, long in_pitch,
                                                      double* __restrict__ P, float* __restrict__ U, Geom g,
                                                      double* __restrict__ partials,
                                                      const double* __restrict__ mean_prev,
                                                      const cx<T>* __restrict__ tw_half,
-                                                     const cx<T>* __restrict__ tw_n, const int* __restrict__ skip)
+                                                     const cx<T>* __restrict__ tw_n, const int* __restrict__ skip,
+                                                     int* __restrict__ err)
 {
     if (skip && *skip) return;
     constexpr int NC = SH::N, W = SH::W, NT = SH::NT;
     constexpr int NR = NC + 1;
-    constexpr int ER = NR * W;
+    constexpr int RS = xinv_rs(NC);                       // BULK: raw row stride
+    constexpr unsigned RB = (unsigned)((NC + 2) * sizeof(cx<T>));   // BULK: bytes per row copy
+    static_assert(!BULK || (NC % 2 == 0 && RS >= NC + 2 && RS * W >= NC * W), "bulk rows");
+    constexpr int ER = BULK ? RS * W : NR * W;
     constexpr int NX = 2 * NC;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cx<T>* cur = reinterpret_cast<cx<T>*>(smem_raw);
     cx<T>* nxt = cur + ER;
     __shared__ long line_base[W], line_gy[W], line_gz[W];
+    __shared__ __align__(8) uint64_t xbar[2];
+    __shared__ int xabort;
     const long nlines = (long)g.ny * g.nz;
     const long ntiles = (nlines + W - 1) / W;
+    if (BULK) {
+        if (threadIdx.x == 0) {
+            mbar_init(&xbar[0], 1);
+            mbar_init(&xbar[1], 1);
+            mbar_init_fence();
+            xabort = 0;
+        }
+        __syncthreads();
+    }
+    int cb = 0;            // BULK: the barrier of the current buffer
+    unsigned xpar = 0;     // BULK: bit b, parity of buffer b's next completion
     auto src = [&](long o) -> double {
         if constexpr (UK == U_ACC) return (double)U[o];
         else return P[o];
@@ -96,25 +133,34 @@ __global__ void __launch_bounds__(SH::NT, (SH::N == 384 || SH::N <= 128) ? 2 : 0
         if constexpr (UK == U_WRITE) U[o] = (float)v;
         else P[o] = v;
     };
-    auto issue = [&](long t, cx<T>* b) {
+    auto issue = [&](long t, cx<T>* b, int bi) {
         const long line0 = t * W;
-        for (int e = threadIdx.x; e < ER; e += NT) {
-            const int l = e / NR, k = e - l * NR;
-            cx<T>* d = b + sidx_ct<T, W, SH::N>(k, l);
-            if (line0 + l < nlines) cp_async_elem(d, in + (line0 + l) * in_pitch + k);
-            else *d = mk<T>((T)0, (T)0);
+        if constexpr (BULK) {
+            if (threadIdx.x == 0) {
+                const int nl = (int)(nlines - line0 < W ? nlines - line0 : W);
+                fence_proxy_async_smem();   // the previous tile's reads of b come first
+                mbar_arrive_expect_tx(&xbar[bi], (unsigned)nl * RB);
+                for (int l = 0; l < nl; ++l) bulk_load(b + l * RS, in + (line0 + l) * in_pitch, RB, &xbar[bi]);
+            }
+        } else {
+            for (int e = threadIdx.x; e < ER; e += NT) {
+                const int l = e / NR, k = e - l * NR;
+                cx<T>* d = b + sidx_ct<T, W, SH::N>(k, l);
+                if (line0 + l < nlines) cp_async_elem(d, in + (line0 + l) * in_pitch + k);
+                else *d = mk<T>((T)0, (T)0);
+            }
+            cp_async_commit();
         }
-        cp_async_commit();
     };
     double acc_du = 0.0, acc_u = 0.0, acc_s = 0.0;
     const double mprev = (ACC && mean_prev) ? *mean_prev : 0.0;
     long t = blockIdx.x;
-    if (t < ntiles) issue(t, cur);
+    if (t < ntiles) issue(t, cur, cb);
     for (; t < ntiles; t += gridDim.x) {
         const long line0 = t * W;
         const long tn = t + gridDim.x;
-        if (tn < ntiles) issue(tn, nxt);
-        else cp_async_commit();
+        if (tn < ntiles) issue(tn, nxt, cb ^ 1);
+        else if (!BULK) cp_async_commit();
         // this tile's rows of u into L2 ahead of the read-modify-write
         if (ACC && threadIdx.x < W && line0 + threadIdx.x < nlines) {
             const long line = line0 + threadIdx.x;
@@ -139,15 +185,29 @@ __global__ void __launch_bounds__(SH::NT, (SH::N == 384 || SH::N <= 128) ? 2 : 0
                 has_yz |= (line < nlines) && (gy || gz);
             }
         }
-        cp_async_wait<1>();  // this thread's copies of tile t have landed
+        if constexpr (BULK) {
+            // the rows of tile t have landed (every thread observes the barrier)
+            if (!mbar_wait_sleep_bounded(&xbar[cb], (xpar >> cb) & 1u, XB_POLL_NS, XB_WAIT_LIMIT)) xabort = 1;
+            xpar ^= 1u << cb;
+        } else {
+            cp_async_wait<1>();  // this thread's copies of tile t have landed
+        }
         // whether any line of the tile has y or z ghosts (most tiles have none)
         const bool yz = __syncthreads_or(has_yz);
+        if (BULK && xabort) {
+            if (threadIdx.x == 0 && err) atomicOr(err, 2);
+            // the next tile's rows may be in flight: wait for them (bounded)
+            // before the CTA's shared memory is released
+            if (threadIdx.x == 0 && tn < ntiles)
+                mbar_wait_sleep_bounded(&xbar[cb ^ 1], (xpar >> (cb ^ 1)) & 1u, XB_POLL_NS, XB_WAIT_LIMIT);
+            break;
+        }
         // the C2R split, Z_m from (X_m, conj X_{nc-m}) with w_m, formed as the
         // first FFT pass loads its inputs (X_0 and X_nc enter with zero
         // imaginary parts)
         auto zsplit = [&](int m, int l) -> cx<T> {
-            cx<T> a = cur[sidx_ct<T, W, SH::N>(m, l)];
-            cx<T> xc = cur[sidx_ct<T, W, SH::N>(NC - m, l)];
+            cx<T> a = BULK ? cur[l * RS + m] : cur[sidx_ct<T, W, SH::N>(m, l)];
+            cx<T> xc = BULK ? cur[l * RS + NC - m] : cur[sidx_ct<T, W, SH::N>(NC - m, l)];
             if (m == 0) { a.y = (T)0; xc.y = (T)0; }
             const cx<T> b = conj(xc);
             const cx<T> Ev = a + b, D = a - b;
@@ -202,6 +262,7 @@ __global__ void __launch_bounds__(SH::NT, (SH::N == 384 || SH::N <= 128) ? 2 : 0
         cx<T>* tmp = cur;
         cur = nxt;
         nxt = tmp;
+        cb ^= 1;
     }
     if (partials) {
         __shared__ double red[3][32];
@@ -279,9 +340,10 @@ template <typename T>
 cudaError_t launch_xinv(bool dct, const void* in, long in_pitch, double* P, float* U, int ukind, const Geom& g,
                         bool accumulate, bool stencil_ghosts, double* partials, const double* mean_prev,
                         const FftSched& sch, const cx<T>* tw_half, const cx<T>* tw_n, const cx<T>* tw_dct,
-                        const int* skip_flag, cudaStream_t st, long* blocks_used)
+                        const int* skip_flag, cudaStream_t st, long* blocks_used, int* err_bits)
 {
     const int nc = g.nx / 2;
+    int* const ebits = err_bits;
     // the FP32 iterate belongs to the refinement of FP32 spectra: U_WRITE
     // with stencil ghosts and no accumulate, U_ACC with both
     if (ukind != U_P && (sizeof(T) != 4 || !U || !stencil_ghosts || accumulate != (ukind == U_ACC)))
@@ -304,22 +366,36 @@ cudaError_t launch_xinv(bool dct, const void* in, long in_pitch, double* P, floa
         };
         if constexpr (SH::CT && sizeof(T) == 4) {
             if (!dct) {  // pipelined FP32 tiles
-                auto pipe = [&](auto kern) {
-                    const size_t psmem = 2 * (size_t)(SH::N + 1) * SH::W * sizeof(cx<T>);
+                auto pipe = [&](auto kern, bool bulk) {
+                    const size_t rows = bulk ? (size_t)xinv_rs(SH::N) : (size_t)(SH::N + 1);
+                    const size_t psmem = 2 * rows * SH::W * sizeof(cx<T>);
                     err = set_smem(kern, psmem);
                     unsigned pgrid = 0;
                     if (err == cudaSuccess) err = persistent_grid(kern, SH::NT, psmem, (long)grid.x, &pgrid);
                     if (err != cudaSuccess) return;
                     if (blocks_used) *blocks_used = pgrid;
                     kern<<<pgrid, SH::NT, psmem, st>>>(reinterpret_cast<const cx<T>*>(in), in_pitch, P, U, g,
-                                                      partials, mean_prev, tw_half, tw_n, skip_flag);
+                                                      partials, mean_prev, tw_half, tw_n, skip_flag, ebits);
                     err = cudaGetLastError();
                 };
-                if (ukind == U_WRITE) pipe(k_xinv_pipe<T, false, true, SH, U_WRITE>);
-                else if (ukind == U_ACC) pipe(k_xinv_pipe<T, true, true, SH, U_ACC>);
-                else if (!stencil_ghosts) pipe(k_xinv_pipe<T, false, false, SH>);
-                else if (accumulate) pipe(k_xinv_pipe<T, true, true, SH>);
-                else pipe(k_xinv_pipe<T, false, true, SH>);
+                // bulk row copies where every row starts on a 16-byte boundary
+                // and the pitch holds the NC + 2 values a copy reads
+                const bool bulk = PPF_XINV_BULK && in_pitch >= SH::N + 2 && (in_pitch * sizeof(cx<T>)) % 16 == 0 &&
+                                  ((uintptr_t)in & 15) == 0;
+                auto pick = [&](auto k_bulk, auto k_elem) {
+                    if (bulk) pipe(k_bulk, true);
+                    else pipe(k_elem, false);
+                };
+                if (ukind == U_WRITE)
+                    pick(k_xinv_pipe<T, false, true, SH, U_WRITE, true>, k_xinv_pipe<T, false, true, SH, U_WRITE, false>);
+                else if (ukind == U_ACC)
+                    pick(k_xinv_pipe<T, true, true, SH, U_ACC, true>, k_xinv_pipe<T, true, true, SH, U_ACC, false>);
+                else if (!stencil_ghosts)
+                    pick(k_xinv_pipe<T, false, false, SH, U_P, true>, k_xinv_pipe<T, false, false, SH, U_P, false>);
+                else if (accumulate)
+                    pick(k_xinv_pipe<T, true, true, SH, U_P, true>, k_xinv_pipe<T, true, true, SH, U_P, false>);
+                else
+                    pick(k_xinv_pipe<T, false, true, SH, U_P, true>, k_xinv_pipe<T, false, true, SH, U_P, false>);
                 return;
             }
         }
@@ -382,7 +458,7 @@ template long xinv_blocks<float>(const Geom&, const FftSched&);
     template cudaError_t launch_xinv<T>(bool, const void*, long, double*, float*, int, const Geom&, bool,  \
                                         bool,                                                              \
                                         double*, const double*, const FftSched&, const cx<T>*,             \
-                                        const cx<T>*, const cx<T>*, const int*, cudaStream_t, long*);
+                                        const cx<T>*, const cx<T>*, const int*, cudaStream_t, long*, int*);
 PPF_INST(double)
 PPF_INST(float)
 #undef PPF_INST
