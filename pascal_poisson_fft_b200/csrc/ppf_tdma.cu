@@ -323,7 +323,7 @@ __device__ __forceinline__ float rcp_approx(float x)
 }
 
 struct ZStream {
-    static constexpr int W = 224;        // columns per block and box row
+    static constexpr int W = 256;        // columns per block and box row (a TMA box holds at most 256)
     static constexpr int NC = 2 * W;     // consumer threads: lower half, upper half of each column
     static constexpr int NT = NC + 32;   // + the producer warp
     static constexpr int R = 16;         // rows per box and checkpoint chunk

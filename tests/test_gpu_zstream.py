@@ -1,6 +1,6 @@
 """The streamed FP32 z solve (k_thomas_stream: TMA ring, twisted sweep per
 column, chunk checkpoints in shared memory), at sizes where a standalone
-plan uses it -- at least one block of 224 FP32 values of a z row per SM
+plan uses it -- at least one block of 256 FP32 values of a z row per SM
 (148 blocks) -- and in the shapes it has to handle: complex columns (real
 and imaginary parts of periodic-x spectra), real columns (DCT x and y), an
 odd number of 16-row chunks with a partial last one, and a single chunk.
@@ -19,7 +19,7 @@ pytestmark = pytest.mark.gpu
 TOL_MIXED = 1e-10
 TOL_FP32 = 5e-5
 
-# (n1m, n2m, n3m, pbc, beta): z rows of ~70k-131k FP32 values (311-585 blocks)
+# (n1m, n2m, n3m, pbc, beta): z rows of ~74k-147k FP32 values (288-576 blocks)
 CASES = [
     (256, 256, 200, (1, 1, 0), 1.5),   # complex; 13 chunks (6 lower, 7 upper), the last 8 rows
     (512, 256, 64, (0, 0, 0), 0.0),    # real columns (DCT x and y); 4 chunks
