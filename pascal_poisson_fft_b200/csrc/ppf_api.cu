@@ -403,7 +403,7 @@ int run_pass(ppf_plan* p, const double* f, double* P, bool resid, bool accumulat
     const long a_cp = p->xdct ? p->a_pitch / 2 : p->a_pitch;
     const long b_cp = (p->xdct && p->ydct) ? p->b_pitch / 2 : p->b_pitch;
     e = launch_yfwd<T>(p->ykind, reinterpret_cast<const cx<T>*>(p->A), a_cp, reinterpret_cast<cx<T>*>(p->B), b_cp,
-                       p->ycols, p->g, p->sy, tyn, tyd, skip, st);
+                       p->ycols, p->g, p->sy, tyn, tyd, skip, st, p->flags + 2);
     if (e != cudaSuccess) return cuda_fail(e, "y forward");
     mark(p, 2, st);
     const ZStreams zs{ st, p->aux, p->ev_fork, p->ev_join };
@@ -412,7 +412,7 @@ int run_pass(ppf_plan* p, const double* f, double* P, bool resid, bool accumulat
     if (e != cudaSuccess) return cuda_fail(e, "z tridiagonal");
     mark(p, 3, st);
     e = launch_yinv<T>(p->ykind, reinterpret_cast<const cx<T>*>(p->B), b_cp, reinterpret_cast<cx<T>*>(p->A), a_cp,
-                       p->ycols, p->g, p->sy, tyn, tyd, p->scal + 4, skip, st);
+                       p->ycols, p->g, p->sy, tyn, tyd, p->scal + 4, skip, st, p->flags + 2);
     if (e != cudaSuccess) return cuda_fail(e, "y inverse");
     mark(p, 4, st);
     // the mixed path keeps the stencil's ghost cells current for its residual

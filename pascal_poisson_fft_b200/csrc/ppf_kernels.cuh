@@ -34,13 +34,14 @@ cudaError_t launch_xfwd(bool dct, const double* f, const ResidIn* resid, const G
 template <typename T>
 cudaError_t launch_yfwd(int kind, const cx<T>* in, long in_pitch, cx<T>* out, long out_pitch,
                         int ncols, const Geom& g, const FftSched& sch,
-                        const cx<T>* tw_ny, const cx<T>* tw_dct, const int* skip_flag, cudaStream_t st);
+                        const cx<T>* tw_ny, const cx<T>* tw_dct, const int* skip_flag, cudaStream_t st,
+                        int* err = nullptr);
 
 template <typename T>
 cudaError_t launch_yinv(int kind, const cx<T>* in, long in_pitch, cx<T>* out, long out_pitch,
                         int ncols, const Geom& g, const FftSched& sch,
                         const cx<T>* tw_ny, const cx<T>* tw_dct, const double* dc_shift,
-                        const int* skip_flag, cudaStream_t st);
+                        const int* skip_flag, cudaStream_t st, int* err = nullptr);
 
 // Where the x inverse reads and writes the iterate of a mixed solve.  The
 // first iterate is made of FP32 values, so when a refinement sweep follows it

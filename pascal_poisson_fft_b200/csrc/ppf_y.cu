@@ -10,7 +10,12 @@
 //            real N-N case with adjacent kx columns packed as complex)
 //   Y_RPAIR: real FFT of two packed real columns (DCT-x data, periodic y);
 //            ny/2+1 rows of two complex columns per packed pair
+#include "ppf_tma.cuh"
 #include "ppf_y_dev.cuh"
+
+#ifndef PPF_Y_TMA
+#define PPF_Y_TMA 1
+#endif
 
 namespace ppf {
 
@@ -128,6 +133,95 @@ __device__ __forceinline__ void y_c2c_pipe(const cx<T>* __restrict__ in, long in
     }
 }
 
+// The paired FP32 pipeline with its tiles loaded by TMA: thread 0 issues the
+// boxes of the next tile (16 columns x up to 256 rows each, one row of a
+// box = one unswizzled 128-byte tile row; columns past ncols read as zero)
+// onto that buffer's mbarrier, every thread waits on the current buffer's
+// barrier (bounded: about 2 s of sleeping polls, then err bit 2 and the
+// CTA stops), and the transform and stores are those of
+// y_c2c_pipe<float, INV, SH, true>.  The tensor map covers this GPU's
+// spectrum only (rows of 2 ncols FP32 values, in_pitch complex apart).
+constexpr unsigned YT_POLL_NS = 20000;
+constexpr long YT_WAIT_LIMIT = 100000;
+
+template <bool INV, typename SH>
+__global__ void __launch_bounds__(SH::NT, 1) k_y_c2c_tma(const __grid_constant__ CUtensorMap tmap,
+                                                     cx<float>* __restrict__ out, long out_pitch, int ncols, int nz,
+                                                     const cx<float>* __restrict__ tw,
+                                                     const double* __restrict__ dc_shift,
+                                                     const int* __restrict__ skip, int* __restrict__ err)
+{
+    if (skip && *skip) return;
+    using T = float;
+    constexpr int N = SH::N, W = SH::W;
+    static_assert(W == 16, "paired 16-column tiles");
+    constexpr int BR = N < 256 ? N : 256;   // rows per box
+    static_assert(N % BR == 0, "whole boxes per tile");
+    constexpr unsigned TILE_BYTES = (unsigned)(N * W * sizeof(cx<T>));
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    // TMA destinations start on 128-byte boundaries: the dynamic region is
+    // rounded up (the launch adds 128 bytes for it)
+    cx<T>* cur = reinterpret_cast<cx<T>*>(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
+    cx<T>* nxt = cur + N * W;
+    __shared__ __align__(8) uint64_t ybar[2];
+    __shared__ int yabort;
+    if (threadIdx.x == 0) {
+        mbar_init(&ybar[0], 1);
+        mbar_init(&ybar[1], 1);
+        mbar_init_fence();
+        yabort = 0;
+    }
+    __syncthreads();
+    const int nblk = (ncols + W - 1) / W;
+    const long ntiles = (long)nblk * nz;
+    const uint64_t pol = l2_policy_evict_first();   // every value is read once
+    auto issue = [&](long t, cx<T>* b, int bi) {
+        if (threadIdx.x == 0) {
+            const int z = (int)(t / nblk), col0 = (int)(t - (long)z * nblk) * W;
+            fence_proxy_async_smem();   // the previous tile's reads of b come first
+            mbar_arrive_expect_tx(&ybar[bi], TILE_BYTES);
+#pragma unroll
+            for (int q = 0; q < N / BR; ++q)
+                tma_load_2d(b + q * BR * W, &tmap, 2 * col0, z * N + q * BR, &ybar[bi], pol);
+        }
+    };
+    int cb = 0;
+    unsigned par = 0;
+    long t = blockIdx.x;
+    if (t < ntiles) issue(t, cur, 0);
+    for (; t < ntiles; t += gridDim.x) {
+        const long tn = t + gridDim.x;
+        if (tn < ntiles) issue(tn, nxt, cb ^ 1);
+        if (!mbar_wait_sleep_bounded(&ybar[cb], (par >> cb) & 1u, YT_POLL_NS, YT_WAIT_LIMIT)) yabort = 1;
+        par ^= 1u << cb;
+        const int z = (int)(t / nblk), col0 = (int)(t - (long)z * nblk) * W;
+        // the zero mode's z-average, removed from the (kx,ky) = (0,0) coefficient
+        if (INV && dc_shift && col0 == 0 && threadIdx.x == 0) cur[0].x -= (T)*dc_shift;
+        __syncthreads();
+        if (yabort) {
+            if (threadIdx.x == 0) {
+                if (err) atomicOr(err, 2);
+                // the next tile's boxes may be in flight: wait for them (bounded)
+                if (tn < ntiles)
+                    mbar_wait_sleep_bounded(&ybar[cb ^ 1], (par >> (cb ^ 1)) & 1u, YT_POLL_NS, YT_WAIT_LIMIT);
+            }
+            break;
+        }
+        cx<T>* outp = out + (long)z * N * out_pitch + col0;
+        auto yst2 = [&](int k, int p, cx<T> u, cx<T> v) {
+            cx<T>* o = outp + (long)k * out_pitch + 2 * p;
+            const int c = col0 + 2 * p;
+            if (c + 1 < ncols) *reinterpret_cast<float4*>(o) = make_float4(u.x, u.y, v.x, v.y);
+            else if (c < ncols) *o = u;
+        };
+        SH::template fft_pair_st<INV>(cur, tw, yst2);
+        cx<T>* tmp = cur;
+        cur = nxt;
+        nxt = tmp;
+        cb ^= 1;
+    }
+}
+
 // FP32 tiles: one CTA per SM (two 64 KB buffers at 512 threads)
 template <typename T, bool INV, typename SH, bool PAIR>
 __global__ void __launch_bounds__(SH::NT) k_y_c2c_pipe(const cx<T>* __restrict__ in, long in_pitch,
@@ -165,8 +259,31 @@ struct PipeShape<double, ShapeCT<N, W, 512, RS...>> {
 
 template <typename T, bool INV, typename SH>
 cudaError_t launch_y_c2c_pipe(const cx<T>* in, long in_pitch, cx<T>* out, long out_pitch, int ncols, int nz,
-                              const cx<T>* tw, const double* dc_shift, const int* skip_flag, cudaStream_t st)
+                              const cx<T>* tw, const double* dc_shift, const int* skip_flag, cudaStream_t st,
+                              int* err)
 {
+    if constexpr (sizeof(T) == 4 && SH::W == 16 && (SH::N <= 256 || SH::N % 256 == 0)) {
+        // TMA-fed paired tiles where the map can describe the spectrum
+        CUtensorMap map;
+        const bool tma = PPF_Y_TMA && ((uintptr_t)in & 15) == 0 && ((uintptr_t)out & 15) == 0 && in_pitch % 2 == 0 &&
+                         out_pitch % 2 == 0 &&
+                         tma_map_2d_f32(&map, const_cast<cx<T>*>(in), 2ull * (unsigned long long)ncols,
+                                        (unsigned long long)nz * SH::N, (unsigned long long)in_pitch * sizeof(cx<T>),
+                                        32u, (unsigned)(SH::N < 256 ? SH::N : 256));
+        if (tma) {
+            auto kern = k_y_c2c_tma<INV, SH>;
+            const size_t smem = 2 * (size_t)SH::N * SH::W * sizeof(cx<T>) + 128;
+            cudaError_t e = set_smem(kern, smem);
+            if (e != cudaSuccess) return e;
+            const long tiles = (long)((ncols + SH::W - 1) / SH::W) * nz;
+            unsigned grid = 0;
+            e = persistent_grid(kern, SH::NT, smem, tiles, &grid);
+            if (e != cudaSuccess) return e;
+            kern<<<grid, SH::NT, smem, st>>>(map, reinterpret_cast<cx<float>*>(out), out_pitch, ncols, nz,
+                                            reinterpret_cast<const cx<float>*>(tw), dc_shift, skip_flag, err);
+            return cudaGetLastError();
+        }
+    }
     // paired passes where the tile is 16 FP32 columns and every column pair
     // starts on a 16-byte boundary
     constexpr bool PAIRABLE = sizeof(T) == 4 && SH::W == PAIR_W;
@@ -191,7 +308,7 @@ cudaError_t launch_y_c2c_pipe(const cx<T>* in, long in_pitch, cx<T>* out, long o
 template <typename T>
 cudaError_t launch_yfwd(int kind, const cx<T>* in, long in_pitch, cx<T>* out, long out_pitch, int ncols,
                         const Geom& g, const FftSched& sch, const cx<T>* tw_ny, const cx<T>* tw_dct,
-                        const int* skip_flag, cudaStream_t st)
+                        const int* skip_flag, cudaStream_t st, int* err_bits)
 {
     cudaError_t err = cudaSuccess;
     with_shape<T>(sch, [&](auto sh) {
@@ -212,7 +329,7 @@ cudaError_t launch_yfwd(int kind, const cx<T>* in, long in_pitch, cx<T>* out, lo
             if constexpr (SH::CT)
                 err = launch_y_c2c_pipe<T, false, typename PipeShape<T, SH>::type>(in, in_pitch, out, out_pitch,
                                                                                   ncols, g.nz, tw_ny, nullptr,
-                                                                                  skip_flag, st);
+                                                                                  skip_flag, st, err_bits);
             else go(k_yfwd<T, Y_C2C, SH>);
         }
         else if (kind == Y_CDCT) go(k_yfwd<T, Y_CDCT, SH>);
@@ -224,7 +341,7 @@ cudaError_t launch_yfwd(int kind, const cx<T>* in, long in_pitch, cx<T>* out, lo
 template <typename T>
 cudaError_t launch_yinv(int kind, const cx<T>* in, long in_pitch, cx<T>* out, long out_pitch, int ncols,
                         const Geom& g, const FftSched& sch, const cx<T>* tw_ny, const cx<T>* tw_dct,
-                        const double* dc_shift, const int* skip_flag, cudaStream_t st)
+                        const double* dc_shift, const int* skip_flag, cudaStream_t st, int* err_bits)
 {
     cudaError_t err = cudaSuccess;
     with_shape<T>(sch, [&](auto sh) {
@@ -245,7 +362,7 @@ cudaError_t launch_yinv(int kind, const cx<T>* in, long in_pitch, cx<T>* out, lo
             if constexpr (SH::CT)
                 err = launch_y_c2c_pipe<T, true, typename PipeShape<T, SH>::type>(in, in_pitch, out, out_pitch,
                                                                                  ncols, g.nz, tw_ny, dc_shift,
-                                                                                 skip_flag, st);
+                                                                                 skip_flag, st, err_bits);
             else go(k_yinv<T, Y_C2C, SH>);
         }
         else if (kind == Y_CDCT) go(k_yinv<T, Y_CDCT, SH>);
@@ -257,10 +374,10 @@ cudaError_t launch_yinv(int kind, const cx<T>* in, long in_pitch, cx<T>* out, lo
 #define PPF_INST(T)                                                                                        \
     template cudaError_t launch_yfwd<T>(int, const cx<T>*, long, cx<T>*, long, int, const Geom&,           \
                                         const FftSched&, const cx<T>*, const cx<T>*, const int*,           \
-                                        cudaStream_t);                                                     \
+                                        cudaStream_t, int*);                                               \
     template cudaError_t launch_yinv<T>(int, const cx<T>*, long, cx<T>*, long, int, const Geom&,           \
                                         const FftSched&, const cx<T>*, const cx<T>*, const double*,        \
-                                        const int*, cudaStream_t);
+                                        const int*, cudaStream_t, int*);
 PPF_INST(double)
 PPF_INST(float)
 #undef PPF_INST
