@@ -377,19 +377,19 @@ __device__ __forceinline__ void fft_ct_last_st(cx<T>* s, const cx<T>* __restrict
 }
 
 // ---------------------------------------------------------------------------
-// Paired passes: FP32 tiles of 16 lines, whose rows are one 128-byte bank
-// row.  A thread takes the butterflies of lines 2p and 2p + 1 at one
-// position, so one 16-byte shared access moves the values of both lines and
-// one set of twiddle powers serves both (the same operations per line as
-// fft_pass_ct).  Element (n, l) sits at n * 16 + l, unswizzled: a warp's
-// accesses cover four whole rows, which is free of bank conflicts.
+// Paired passes: FP32 tiles of W lines (W even; 16 or 8: rows of one or
+// half a 128-byte bank row).  A thread takes the butterflies of lines 2p and
+// 2p + 1 at one position, so one 16-byte shared access moves the values of
+// both lines and one set of twiddle powers serves both (the same operations
+// per line as fft_pass_ct).  Element (n, l) sits at n * W + l, unswizzled: a
+// warp's accesses cover whole consecutive rows, or rows R apart in a first
+// pass of odd radix R, which is free of bank conflicts.
 // ---------------------------------------------------------------------------
-constexpr int PAIR_W = 16;
-
-template <bool INV, int N, int NT, int R, int NS, typename ST = TileSt>
+template <bool INV, int N, int W, int NT, int R, int NS, typename ST = TileSt>
 __device__ __forceinline__ void fft_pass_pair(cx<float>* s, const cx<float>* __restrict__ tw, ST st = ST{})
 {
-    constexpr int P = PAIR_W / 2;
+    static_assert(W % 2 == 0, "paired tiles hold an even number of lines");
+    constexpr int P = W / 2;
     constexpr int NB = N / R;
     constexpr int ITEMS = NB * P;
     constexpr int Q = (ITEMS + NT - 1) / NT;
@@ -449,14 +449,14 @@ __device__ __forceinline__ void fft_pass_pair(cx<float>* s, const cx<float>* __r
 
 // Every paired pass of a radix sequence, the last one handing outputs n of
 // lines 2p and 2p + 1 to st(n, p, u, v) instead of the tile
-template <bool INV, int N, int NT, int NS, typename ST, int R0, int... RS>
+template <bool INV, int N, int W, int NT, int NS, typename ST, int R0, int... RS>
 __device__ __forceinline__ void fft_pair_last_st(cx<float>* s, const cx<float>* __restrict__ tw, ST st)
 {
     if constexpr (sizeof...(RS) == 0) {
-        fft_pass_pair<INV, N, NT, R0, NS, ST>(s, tw, st);
+        fft_pass_pair<INV, N, W, NT, R0, NS, ST>(s, tw, st);
     } else {
-        fft_pass_pair<INV, N, NT, R0, NS>(s, tw);
-        fft_pair_last_st<INV, N, NT, NS * R0, ST, RS...>(s, tw, st);
+        fft_pass_pair<INV, N, W, NT, R0, NS>(s, tw);
+        fft_pair_last_st<INV, N, W, NT, NS * R0, ST, RS...>(s, tw, st);
     }
 }
 
@@ -493,13 +493,12 @@ struct ShapeCT {
     {
         fft_ct_chain<T, INV, N_, W_, NT_, 1, true, LD, ST, RS...>(s, tw, ld, st);
     }
-    // fft_st in paired passes (FP32, W = PAIR_W): st(n, p, u, v) receives
+    // fft_st in paired passes (FP32, W even): st(n, p, u, v) receives
     // outputs n of lines 2p and 2p + 1
     template <bool INV, typename ST>
     static __device__ __forceinline__ void fft_pair_st(cx<float>* s, const cx<float>* __restrict__ tw, ST st)
     {
-        static_assert(W_ == PAIR_W, "paired passes take 16-line tiles");
-        fft_pair_last_st<INV, N_, NT_, 1, ST, RS...>(s, tw, st);
+        fft_pair_last_st<INV, N_, W_, NT_, 1, ST, RS...>(s, tw, st);
     }
 };
 

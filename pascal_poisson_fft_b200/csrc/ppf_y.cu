@@ -16,6 +16,14 @@
 #ifndef PPF_Y_TMA
 #define PPF_Y_TMA 1
 #endif
+// tile widths of the paired passes (16 columns: 512-point lines; 8: 768)
+#ifndef PPF_Y_PAIR8
+#define PPF_Y_PAIR8 1
+#endif
+// tile widths loaded by TMA
+#ifndef PPF_Y_TMA_W
+#define PPF_Y_TMA_W(w) ((w) == 16 || (PPF_Y_PAIR8 && (w) == 8))
+#endif
 
 namespace ppf {
 
@@ -59,7 +67,7 @@ __device__ __forceinline__ void y_c2c_pipe(const cx<T>* __restrict__ in, long in
     constexpr int LGW = ct_log2y(W);
     constexpr int EPT = (N * W) / NT;
     static_assert(EPT * NT == N * W, "tile elements must divide over the threads");
-    static_assert(!PAIR || (sizeof(T) == 4 && W == PAIR_W && EPT % 2 == 0), "paired tiles: FP32, 16 columns");
+    static_assert(!PAIR || (sizeof(T) == 4 && W % 2 == 0 && EPT % 2 == 0), "paired tiles: FP32, an even width");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cx<T>* cur = reinterpret_cast<cx<T>*>(smem_raw);
     cx<T>* nxt = cur + N * W;
@@ -134,8 +142,8 @@ __device__ __forceinline__ void y_c2c_pipe(const cx<T>* __restrict__ in, long in
 }
 
 // The paired FP32 pipeline with its tiles loaded by TMA: thread 0 issues the
-// boxes of the next tile (16 columns x up to 256 rows each, one row of a
-// box = one unswizzled 128-byte tile row; columns past ncols read as zero)
+// boxes of the next tile (W columns x up to 256 rows each, one row of a
+// box = one unswizzled tile row of 8W bytes; columns past ncols read as zero)
 // onto that buffer's mbarrier, every thread waits on the current buffer's
 // barrier (bounded: about 2 s of sleeping polls, then err bit 2 and the
 // CTA stops), and the transform and stores are those of
@@ -143,6 +151,8 @@ __device__ __forceinline__ void y_c2c_pipe(const cx<T>* __restrict__ in, long in
 // spectrum only (rows of 2 ncols FP32 values, in_pitch complex apart).
 constexpr unsigned YT_POLL_NS = 20000;
 constexpr long YT_WAIT_LIMIT = 100000;
+
+template <int W> struct PairWidth { static constexpr bool value = W == 16 || (PPF_Y_PAIR8 && W == 8); };
 
 template <bool INV, typename SH>
 __global__ void __launch_bounds__(SH::NT, 1) k_y_c2c_tma(const __grid_constant__ CUtensorMap tmap,
@@ -154,7 +164,7 @@ __global__ void __launch_bounds__(SH::NT, 1) k_y_c2c_tma(const __grid_constant__
     if (skip && *skip) return;
     using T = float;
     constexpr int N = SH::N, W = SH::W;
-    static_assert(W == 16, "paired 16-column tiles");
+    static_assert(W % 2 == 0, "paired tiles of an even width");
     constexpr int BR = N < 256 ? N : 256;   // rows per box
     static_assert(N % BR == 0, "whole boxes per tile");
     constexpr unsigned TILE_BYTES = (unsigned)(N * W * sizeof(cx<T>));
@@ -262,14 +272,15 @@ cudaError_t launch_y_c2c_pipe(const cx<T>* in, long in_pitch, cx<T>* out, long o
                               const cx<T>* tw, const double* dc_shift, const int* skip_flag, cudaStream_t st,
                               int* err)
 {
-    if constexpr (sizeof(T) == 4 && SH::W == 16 && (SH::N <= 256 || SH::N % 256 == 0)) {
+    if constexpr (sizeof(T) == 4 && PairWidth<SH::W>::value && PPF_Y_TMA_W(SH::W) &&
+                  (SH::N <= 256 || SH::N % 256 == 0)) {
         // TMA-fed paired tiles where the map can describe the spectrum
         CUtensorMap map;
         const bool tma = PPF_Y_TMA && ((uintptr_t)in & 15) == 0 && ((uintptr_t)out & 15) == 0 && in_pitch % 2 == 0 &&
                          out_pitch % 2 == 0 &&
                          tma_map_2d_f32(&map, const_cast<cx<T>*>(in), 2ull * (unsigned long long)ncols,
                                         (unsigned long long)nz * SH::N, (unsigned long long)in_pitch * sizeof(cx<T>),
-                                        32u, (unsigned)(SH::N < 256 ? SH::N : 256));
+                                        2u * SH::W, (unsigned)(SH::N < 256 ? SH::N : 256));
         if (tma) {
             auto kern = k_y_c2c_tma<INV, SH>;
             const size_t smem = 2 * (size_t)SH::N * SH::W * sizeof(cx<T>) + 128;
@@ -286,7 +297,7 @@ cudaError_t launch_y_c2c_pipe(const cx<T>* in, long in_pitch, cx<T>* out, long o
     }
     // paired passes where the tile is 16 FP32 columns and every column pair
     // starts on a 16-byte boundary
-    constexpr bool PAIRABLE = sizeof(T) == 4 && SH::W == PAIR_W;
+    constexpr bool PAIRABLE = sizeof(T) == 4 && PairWidth<SH::W>::value;
     const bool pair = PAIRABLE && in_pitch % 2 == 0 && out_pitch % 2 == 0 && ((uintptr_t)in & 15) == 0 &&
                       ((uintptr_t)out & 15) == 0;
     auto kern = [&] {
