@@ -90,7 +90,7 @@ constexpr unsigned XB_POLL_NS = 20000;
 constexpr long XB_WAIT_LIMIT = 100000;
 
 template <typename T, bool ACC, bool GHOST, typename SH, int UK = U_P, bool BULK = false>
-__global__ void __launch_bounds__(SH::NT, (SH::N == 384 || SH::N <= 128) ? 2 : (SH::N == 256 ? PPF_XINV_256_CTAS : 0)) k_xinv_pipe(const cx<T>* __restrict__ in, long in_pitch,
+__global__ void __launch_bounds__(SH::NT, (SH::N <= 128) ? 2 : SH::N == 384 ? 3 : (SH::N == 256 ? PPF_XINV_256_CTAS : 0)) k_xinv_pipe(const cx<T>* __restrict__ in, long in_pitch,
                                                      double* __restrict__ P, float* __restrict__ U, Geom g,
                                                      double* __restrict__ partials,
                                                      const double* __restrict__ mean_prev,
