@@ -29,8 +29,10 @@ namespace ppf {
         const cx<T>* __restrict__ tw_dct, const int* __restrict__ skip
 #define PPF_XFWD_ARGS f, rs, g, out_, out_pitch, sch, Wrt, lgWrt, tw_half, tw_n, tw_dct, skip, (long)blockIdx.x
 
+// the plain periodic transform of 384-point tiles (768-point lines) is bounded
+// to four resident CTAs of 384 threads: 32 registers, five CTAs fit an SM
 template <typename T, bool DCT, int RESID, typename SH>
-__global__ void __launch_bounds__(512) k_xfwd(PPF_XFWD_PARAMS)
+__global__ void __launch_bounds__(512, (SH::N == 384 && !DCT && RESID == 0) ? 4 : 0) k_xfwd(PPF_XFWD_PARAMS)
 {
     xfwd<T, DCT, RESID, SH>(PPF_XFWD_ARGS);
 }
